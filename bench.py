@@ -1,0 +1,435 @@
+#!/usr/bin/env python
+"""FRSZ2 compress/decompress throughput on B200.
+
+Default workload (the configuration the headline metric is quoted on): an fp32
+512^3 field (sum of 8 random-phase plane sinusoids, wavelengths 8-256 cells,
+plus N(0, 1e-3) noise), exponent block 32, 16 bits per value.  One step =
+compress the whole field into its FRSZ2 buffer, then decompress it back.
+
+  value     whole-job GB/s of algorithmic bytes (compress: values read + exps
+            and words written; decompress: the reverse; the 256 B pad is not
+            counted), inputs resident in HBM, timed with CUDA events
+  e2e       the same metric through the C ABI's host-buffer entry points
+            (frsz2_compress_host / frsz2_decompress_host): pinned host buffers,
+            H2D and D2H copies inside the timed region
+  roofline  the dominant kernel's algorithmic GB/s over the measured HBM copy
+            bandwidth
+  cpu_baseline  the reference's own CPU codec (oracle/_ref, all host threads)
+            on a bounded sample of the same workload
+
+``--impl reference`` times that reference CPU codec alone on the same
+workload and prints the reference-arm line.  Under torchrun every rank
+compresses its own field (weak scaling, no data-path collective); the timing
+is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "FRSZ2 compress/decompress GB/s & % HBM peak; batched vs per-array; p50/p99 latency"
+
+WORKLOADS = {
+    # name: (kind, dtype, n, bits, E)
+    "field512_f32_b16_e32": ("field", "float32", 512 ** 3, 16, 32),
+    "loguniform_f64_2p28_b16_e32": ("loguniform", "float64", 1 << 28, 16, 32),
+    "loguniform_f64_2p28_b21_e32": ("loguniform", "float64", 1 << 28, 21, 32),
+    "loguniform_f64_2p28_b32_e32": ("loguniform", "float64", 1 << 28, 32, 32),
+    "loguniform_f64_2p28_b16_e64": ("loguniform", "float64", 1 << 28, 16, 64),
+    "loguniform_f64_2p28_b21_e64": ("loguniform", "float64", 1 << 28, 21, 64),
+    "loguniform_f64_2p28_b32_e64": ("loguniform", "float64", 1 << 28, 32, 64),
+    "normal_f64_2p20_b32_e32": ("normal", "float64", 1 << 20, 32, 32),
+}
+DEFAULT_WORKLOAD = "field512_f32_b16_e32"
+
+# DRAM bytes (read + write) per launch from ncu captures, by (workload, kernel);
+# profiles/ holds the captures' summaries and the commands that made them.
+NCU_TRAFFIC = {}
+
+
+def algorithmic_bytes(dtype: str, n: int, bits: int, E: int) -> int:
+    """Per-launch algorithmic bytes: n values + ceil(n/E) * (block bytes +
+    exponent bytes); identical for compress and decompress."""
+    es = 4 if dtype == "float32" else 8
+    W = 8 if bits <= 8 else 16 if bits <= 16 else 32 if bits <= 32 else 64
+    nb = -(-n // E)
+    block_bytes = -(-E * bits // W) * (W // 8)
+    return n * es + nb * (block_bytes + W // 8)
+
+
+def load_peaks() -> dict:
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return {"hbm_gbs": float(d["hbm_gbs"]), "source": "measured"}
+    return {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
+# ---------------------------------------------------------------- clocks
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            import tempfile
+
+            fd, self.path = tempfile.mkstemp(prefix="frsz2_clocks_", suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "50"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self) -> dict | None:
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                rows.append((float(parts[1]), float(parts[2]), parts[5:9]))
+            except ValueError:
+                continue
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for _, _, r in rows for i, v in enumerate(r) if v.lower() == "active"})
+        return {"sm_mhz": statistics.median(r[0] for r in rows), "sm_max_mhz": max(r[1] for r in rows),
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ---------------------------------------------------------------- inputs
+
+def make_input_cuda(kind: str, dtype: str, n: int, seed: int):
+    import torch
+
+    from frsz_b200 import workloads
+
+    tdt = torch.float32 if dtype == "float32" else torch.float64
+    if kind == "field":
+        side = round(n ** (1 / 3))
+        return workloads.sinusoid_field_cuda(side, side, side, seed=seed, dtype=tdt)
+    if kind == "loguniform":
+        return workloads.loguniform_cuda(n, tdt, seed=seed)
+    return workloads.normal_cuda(n, tdt, seed=seed)
+
+
+def make_input_host_sample(kind: str, dtype: str, n: int, seed: int, sample: int) -> np.ndarray:
+    """The first `sample` values of the workload, generated on the host."""
+    import torch
+
+    from frsz_b200 import workloads
+
+    npdt = np.float32 if dtype == "float32" else np.float64
+    if kind == "field":
+        side = round(n ** (1 / 3))
+        nz = max(1, -(-sample // (side * side)))
+        f = workloads.sinusoid_field_cuda(side, side, nz, seed=seed, dtype=torch.float32, device="cpu")
+        return f.numpy().astype(npdt)[:sample]
+    if kind == "loguniform":
+        return workloads.loguniform_np(sample, npdt, seed=seed)
+    return workloads.normal_np(sample, npdt, seed=seed)
+
+
+# ---------------------------------------------------------------- CPU reference codec
+
+def cpu_reference_codec(x: np.ndarray, bits: int, E: int, threads: int, min_seconds: float):
+    """Time the reference CPU codec (or, where it is not built, the oracle
+    port) on `x`: compress + decompress per rep.  Returns (GB/s, kind, reps)."""
+    import oracle
+
+    kind = "reference" if oracle.ref_available() else "port"
+    buf = np.zeros(oracle.compressed_bytes(bits, E, x.size), dtype=np.uint8)
+    y = np.empty_like(x)
+
+    def rep():
+        if kind == "reference":
+            oracle.ref_compress_into(x, buf, bits, E, threads)
+            oracle.ref_decompress_into(buf, y, bits, E, threads)
+        else:
+            lib = oracle.oracle_lib()
+            lib.frsz2o_compress_mt(int(x.dtype == np.float64), x.ctypes.data, x.size, bits, E, buf.ctypes.data,
+                                   threads)
+            lib.frsz2o_decompress_mt(int(x.dtype == np.float64), buf.ctypes.data, x.size, bits, E, y.ctypes.data,
+                                     threads)
+
+    rep()  # warm
+    reps = 0
+    t0 = time.perf_counter()
+    while True:
+        rep()
+        reps += 1
+        if time.perf_counter() - t0 >= min_seconds:
+            break
+    dt = time.perf_counter() - t0
+    nbytes = 2 * algorithmic_bytes(str(x.dtype), x.size, bits, E)
+    return nbytes * reps / dt / 1e9, kind, reps
+
+
+# ---------------------------------------------------------------- reference arm
+
+def run_reference_arm(args, rank: int, world: int) -> None:
+    if rank != 0:
+        return
+    kind, dtype, n, bits, E = WORKLOADS[args.workload]
+    threads = os.cpu_count() or 1
+    sample = min(n, 1 << 24)
+    x = make_input_host_sample(kind, dtype, n, args.seed, sample)
+    import oracle
+
+    impl_kind = "reference" if oracle.ref_available() else "port"
+    buf = np.zeros(oracle.compressed_bytes(bits, E, x.size), dtype=np.uint8)
+    y = np.empty_like(x)
+
+    def step(xs, b, ys):
+        if impl_kind == "reference":
+            oracle.ref_compress_into(xs, b, bits, E, threads)
+            oracle.ref_decompress_into(b, ys, bits, E, threads)
+        else:
+            lib = oracle.oracle_lib()
+            lib.frsz2o_compress_mt(int(xs.dtype == np.float64), xs.ctypes.data, xs.size, bits, E, b.ctypes.data,
+                                   threads)
+            lib.frsz2o_decompress_mt(int(xs.dtype == np.float64), b.ctypes.data, xs.size, bits, E, ys.ctypes.data,
+                                     threads)
+
+    t0 = time.perf_counter()
+    for _ in range(max(1, args.warmup)):
+        step(x, buf, y)
+    per = (time.perf_counter() - t0) / max(1, args.warmup)
+    # keep the whole timed run within about a minute
+    if per * args.steps > 60.0:
+        sample = max(1 << 18, int(sample * 60.0 / (per * args.steps)) // E * E)
+        x = x[:sample].copy()
+        buf = np.zeros(oracle.compressed_bytes(bits, E, x.size), dtype=np.uint8)
+        y = np.empty_like(x)
+        step(x, buf, y)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        step(x, buf, y)
+    dt = time.perf_counter() - t0
+    nbytes = 2 * algorithmic_bytes(dtype, x.size, bits, E)
+    value = nbytes * args.steps / dt / 1e9
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(value, 3), "unit": "GB/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(dt / args.steps * 1e3, 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "u32" if dtype == "float32" else "u64", "data": "synthetic",
+        "config": {"workload": args.workload, "dtype": dtype, "n": n, "bits": bits, "block_size": E,
+                   "sample_values": int(x.size)},
+        "cpu_baseline": {"value": round(value, 3), "unit": "GB/s", "cores": threads, "kind": impl_kind,
+                         "sample": f"first {x.size} values of the workload, compress+decompress per step"},
+        "e2e": {"value": round(value, 3), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------- our arm
+
+def run_ours(args, rank: int, world: int, local_rank: int) -> None:
+    import torch
+
+    import frsz_b200
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local_rank))
+
+    kind, dtype, n, bits, E = WORKLOADS[args.workload]
+    frsz_b200.lib()  # fail loudly if the library is missing
+    x = make_input_cuda(kind, dtype, n, args.seed + rank)
+    tdt = x.dtype
+    size = frsz_b200.compressed_size(dtype, bits, E, n)
+    buf = torch.zeros(size, dtype=torch.uint8, device="cuda")
+    y = torch.empty_like(x)
+    stream = torch.cuda.current_stream()
+    per_launch = algorithmic_bytes(dtype, n, bits, E)
+    step_bytes = 2 * per_launch
+
+    def step(ev=None):
+        if ev is not None:
+            ev[0].record(stream)
+        frsz_b200.compress(x, bits, E, out=buf, stream=stream)
+        if ev is not None:
+            ev[1].record(stream)
+        frsz_b200.decompress(buf, n, dtype, bits, E, out=y, stream=stream)
+        if ev is not None:
+            ev[2].record(stream)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+
+    K = args.steps
+    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(K)]
+    clocks = ClockSampler(torch.cuda.current_device()) if rank == 0 else None
+    if clocks:
+        clocks.start()
+        time.sleep(0.3)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t_start = torch.cuda.Event(enable_timing=True)
+    t_end = torch.cuda.Event(enable_timing=True)
+    t_start.record(stream)
+    for k in range(K):
+        step(evs[k])
+    t_end.record(stream)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clk = clocks.stop() if clocks else None
+
+    elapsed_ms = t_start.elapsed_time(t_end)
+    comp_ms = [e[0].elapsed_time(e[1]) for e in evs]
+    decomp_ms = [e[1].elapsed_time(e[2]) for e in evs]
+    if dist:
+        t = torch.tensor([elapsed_ms, statistics.mean(comp_ms), statistics.mean(decomp_ms)], device="cuda",
+                         dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        elapsed_ms, comp_avg, decomp_avg = (float(v) for v in t)
+    else:
+        comp_avg, decomp_avg = statistics.mean(comp_ms), statistics.mean(decomp_ms)
+
+    value = world * step_bytes * K / (elapsed_ms / 1e3) / 1e9
+
+    # ---- end to end through the host-buffer C ABI
+    e2e = None
+    if not args.no_e2e:
+        xh = x.cpu().pin_memory()
+        ch = torch.zeros(size, dtype=torch.uint8).pin_memory()
+        yh = torch.empty_like(xh).pin_memory()
+        xn, cn, yn = xh.numpy(), ch.numpy(), yh.numpy()
+        npdt = np.float32 if dtype == "float32" else np.float64
+
+        def e2e_step():
+            frsz_b200.compress_host(xn, bits, E, out=cn)
+            frsz_b200.decompress_host(cn, n, npdt, bits, E, out=yn)
+
+        e2e_step()
+        K2 = max(3, min(K, args.e2e_steps))
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(K2):
+            e2e_step()
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        if dist:
+            t = torch.tensor([dt], device="cuda", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            dt = float(t[0])
+        comp_written = per_launch - n * (4 if dtype == "float32" else 8)
+        e2e = {"value": round(world * step_bytes * K2 / dt / 1e9, 3), "unit": "GB/s",
+               "h2d_bytes_per_step": n * (4 if dtype == "float32" else 8) + comp_written,
+               "d2h_bytes_per_step": comp_written + n * (4 if dtype == "float32" else 8), "steps": K2}
+        if rank == 0:
+            # the host path must agree with the device path
+            assert torch.equal(torch.from_numpy(cn), buf.cpu()), "host-path bytes differ from the device path"
+        del xh, ch, yh
+
+    # ---- CPU baseline: reference codec on the host cores, rank 0 at N = 1
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        sample = min(n, 1 << 24)
+        xs = x[:sample].cpu().numpy()
+        threads = os.cpu_count() or 1
+        gbs, ckind, reps = cpu_reference_codec(xs, bits, E, threads, args.cpu_seconds)
+        cpu = {"value": round(gbs, 3), "unit": "GB/s", "cores": threads, "kind": ckind,
+               "sample": f"first {sample} values of the workload, compress+decompress, {reps} reps"}
+
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+
+    peaks = load_peaks()
+    dom_ms = max(comp_avg, decomp_avg)
+    dom = "compress" if comp_avg >= decomp_avg else "decompress"
+    achieved = per_launch / (dom_ms / 1e3) / 1e9
+    traffic = NCU_TRAFFIC.get((args.workload, dom))
+    line = {
+        "metric": METRIC, "value": round(value, 3), "unit": "GB/s", "n_gpus": world, "steps": K,
+        "warmup": args.warmup, "ms_per_step": round(elapsed_ms / K, 5), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u32" if dtype == "float32" else "u64",
+        "data": "synthetic",
+        "config": {"workload": args.workload, "dtype": dtype, "n": n, "bits": bits, "block_size": E,
+                   "bytes_per_step": step_bytes, "l2": "inputs larger than L2, no flush",
+                   "parallelism": f"replicas x{world}"},
+        "compress_gbs": round(per_launch / (comp_avg / 1e3) / 1e9, 2),
+        "decompress_gbs": round(per_launch / (decomp_avg / 1e3) / 1e9, 2),
+        "compress_ms": round(comp_avg, 5), "decompress_ms": round(decomp_avg, 5),
+        "hbm_frac": {"compress": round(per_launch / (comp_avg / 1e3) / 1e9 / peaks["hbm_gbs"], 4),
+                     "decompress": round(per_launch / (decomp_avg / 1e3) / 1e9 / peaks["hbm_gbs"], 4),
+                     "of": peaks["source"]},
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 2), "peak": peaks["hbm_gbs"],
+                     "unit": "GB/s", "frac": round(achieved / peaks["hbm_gbs"], 4), "traffic": traffic,
+                     "algorithmic_bytes": per_launch, "peak_source": peaks["source"]},
+        "cpu_baseline": cpu,
+        "e2e": e2e,
+        "gpu_launches": 2 * K,
+        "clocks": clk,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default=DEFAULT_WORKLOAD)
+    ap.add_argument("--seed", type=int, default=42)
+    ap.add_argument("--e2e-steps", type=int, default=10)
+    ap.add_argument("--cpu-seconds", type=float, default=3.0)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference_arm(args, rank, world)
+    else:
+        run_ours(args, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    main()

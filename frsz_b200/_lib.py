@@ -1,0 +1,73 @@
+"""ctypes binding of libfrsz2_b200.so (the C ABI declared in include/frsz2_b200.h).
+
+There is no fallback: if the library is missing or fails to load, every call
+raises.  Build it with ``python -m frsz_b200.build`` (or ``__graft_entry__.build()``).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import threading
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libfrsz2_b200.so")
+
+FRSZ2_OK = 0
+FRSZ2_EDTYPE = 1
+FRSZ2_EFAIL = 2
+FRSZ2_FLOAT = 0
+FRSZ2_DOUBLE = 1
+
+_u64 = ctypes.c_uint64
+_vp = ctypes.c_void_p
+_int = ctypes.c_int
+
+# name -> (restype, argtypes); kept in step with include/frsz2_b200.h
+SIGNATURES = {
+    "register_frsz": (None, []),
+    "frsz2_version": (ctypes.c_char_p, []),
+    "frsz2_last_error": (ctypes.c_char_p, []),
+    "frsz2_compressed_size": (_int, [_int, _int, _int, _u64, ctypes.POINTER(_u64)]),
+    "frsz2_exponent_size": (_int, [_int, _int, _int, _u64, ctypes.POINTER(_u64)]),
+    "frsz2_compress": (_int, [_int, _int, _int, _vp, _u64, _vp, _vp]),
+    "frsz2_decompress": (_int, [_int, _int, _int, _vp, _u64, _vp, _vp]),
+    "frsz2_compress_host": (_int, [_int, _int, _int, _vp, _u64, _vp, _vp]),
+    "frsz2_decompress_host": (_int, [_int, _int, _int, _vp, _u64, _vp, _vp]),
+    "frsz2_decompress_elements": (_int, [_int, _int, _int, _vp, _u64, _vp, _u64, _vp, _vp]),
+}
+
+
+class Frsz2Error(RuntimeError):
+    """Non-zero status from the C ABI: 1 = unsupported dtype, 2 = unsupported
+    bits / block size or runtime failure (src/frsz2.cc:164-168 semantics)."""
+
+    def __init__(self, code: int, message: str):
+        super().__init__(message)
+        self.code = code
+
+
+_lock = threading.Lock()
+_handle = None
+
+
+def lib() -> ctypes.CDLL:
+    global _handle
+    if _handle is None:
+        with _lock:
+            if _handle is None:
+                if not os.path.exists(LIB_PATH):
+                    raise RuntimeError(f"{LIB_PATH} is not built; run `python -m frsz_b200.build` "
+                                       "(the FRSZ2 codec has no CPU fallback)")
+                h = ctypes.CDLL(LIB_PATH)
+                for name, (res, args) in SIGNATURES.items():
+                    fn = getattr(h, name)
+                    fn.restype = res
+                    fn.argtypes = args
+                _handle = h
+    return _handle
+
+
+def check(rc: int) -> None:
+    if rc != FRSZ2_OK:
+        msg = lib().frsz2_last_error()
+        raise Frsz2Error(rc, msg.decode() if msg else f"status {rc}")

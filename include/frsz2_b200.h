@@ -1,0 +1,100 @@
+/*
+ * frsz2_b200.h -- C ABI of the B200 FRSZ2 fixed-rate codec (libfrsz2_b200.so).
+ *
+ * Plain pointers and sizes only.  `stream` is a cudaStream_t passed as void*
+ * (NULL = the legacy default stream).  Every entry point returns a status:
+ *
+ *   FRSZ2_OK        0  success
+ *   FRSZ2_EDTYPE    1  unsupported dtype            (src/frsz2.cc:164, 181: set_error(1, "unsupported dtype"))
+ *   FRSZ2_EFAIL     2  unsupported bits / block size, bad argument or CUDA
+ *                      failure                       (src/frsz2.cc:166-168, 183-185: set_error(2, what))
+ *
+ * and frsz2_last_error() gives the calling thread's last message, with the
+ * reference's wording for unsupported values ("Unsupported number of bits: N",
+ * "Unsupported exponent block size: N", include/frsz2.hpp:1300, 1326).
+ *
+ * The compressed format is byte-identical to the reference's
+ * frsz::frsz2_compressor<bits, block_size, T> (include/frsz2.hpp:504-1256):
+ *   [ceil(n/E) exponents, signed W-bit] [pad to next 256 B multiple, full 256 B
+ *   if aligned] [ceil(n/E) blocks of ceil(E*bits/W) W-bit words, LSB-first]
+ * with W = 8/16/32/64 for bits <= 8/16/32/64.  Bytes the reference never
+ * writes (the pad, unused tail words of a partial last block) are left as the
+ * caller's buffer had them.
+ *
+ * Valid arguments: dtype FRSZ2_FLOAT with 4 <= bits <= 32, FRSZ2_DOUBLE with
+ * 4 <= bits <= 64 (static_asserts include/frsz2.hpp:511-517); 1 <= block_size
+ * <= 65536.  Device pointers must be aligned to their element / word type.
+ */
+#ifndef FRSZ2_B200_H
+#define FRSZ2_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FRSZ2_OK 0
+#define FRSZ2_EDTYPE 1
+#define FRSZ2_EFAIL 2
+
+/* Element types: the two dtypes the plugin's compress/decompress switch
+ * accepts (src/frsz2.cc:157-163, 174-179). */
+#define FRSZ2_FLOAT 0
+#define FRSZ2_DOUBLE 1
+
+/* Replaces frsz.h:1 `extern "C" void register_frsz();` (empty body,
+ * src/frsz.cc:11-13): a link anchor kept with the same name and signature. */
+void register_frsz(void);
+
+/* Library version; the plugin reports 0.0.2 (src/frsz2.cc:188-192). */
+const char* frsz2_version(void);
+
+/* Message for the calling thread's last non-zero status. */
+const char* frsz2_last_error(void);
+
+/* Replaces frsz2_compressor<bits,E,T>::compute_compressed_memory_size_byte
+ * (include/frsz2.hpp:542-548) and compute_exponent_block_size_byte
+ * (include/frsz2.hpp:534-540), with bits / E / T chosen at run time. */
+int frsz2_compressed_size(int dtype, int bits, int block_size, uint64_t n, uint64_t* total_bytes);
+int frsz2_exponent_size(int dtype, int bits, int block_size, uint64_t n, uint64_t* exponent_bytes);
+
+/* Device buffers, stream-ordered, asynchronous.
+ * Replaces frsz2_compressor<bits,E,T>::compress_cpu_impl (include/frsz2.hpp:1181-1193)
+ * as reached from dispatch_frsz2_compression (include/frsz2.hpp:1346) and the
+ * plugin's compress_impl (src/frsz2.cc:152-169), and the reference GPU kernel
+ * compress_gpu (include/frsz2.hpp:1259-1274).  `d_compressed` holds
+ * frsz2_compressed_size() bytes. */
+int frsz2_compress(int dtype, int bits, int block_size, const void* d_values, uint64_t n, void* d_compressed,
+                   void* stream);
+
+/* Replaces decompress_cpu_impl (include/frsz2.hpp:1242-1249) via
+ * dispatch_frsz2_decompression (include/frsz2.hpp:1347) and the plugin's
+ * decompress_impl (src/frsz2.cc:171-186), and the reference GPU kernel
+ * decompress_gpu (include/frsz2.hpp:1276-1288). */
+int frsz2_decompress(int dtype, int bits, int block_size, const void* d_compressed, uint64_t n, void* d_values,
+                     void* stream);
+
+/* Host buffers: the same codec with the host<->device copies inside the call
+ * (pinned memory recommended; pageable works).  Synchronous: returns when the
+ * result is in host memory.  This is the drop-in for the reference's host-side
+ * compress_cpu_impl / decompress_cpu_impl calls. */
+int frsz2_compress_host(int dtype, int bits, int block_size, const void* h_values, uint64_t n, void* h_compressed,
+                        void* stream);
+int frsz2_decompress_host(int dtype, int bits, int block_size, const void* h_compressed, uint64_t n, void* h_values,
+                          void* stream);
+
+/* Random-access decode of `count` elements at device indices d_idx[0..count)
+ * into d_out.  Replaces decompress_gpu_element (include/frsz2.hpp:1096-1104)
+ * and decompress_cpu_element (include/frsz2.hpp:1199-1214); values are
+ * bit-exact with the CPU decode (decompress_cpu_element), including the zero
+ * code rule, which the reference GPU element decode does not follow. */
+int frsz2_decompress_elements(int dtype, int bits, int block_size, const void* d_compressed, uint64_t n,
+                              const uint64_t* d_idx, uint64_t count, void* d_out, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FRSZ2_B200_H */

@@ -1,0 +1,116 @@
+"""Regenerate the golden fixtures from the REFERENCE codec.
+
+Runs the reference's own frsz2.hpp (compiled by oracle/Makefile into
+oracle/_ref/libfrsz2_ref.so) on seeded inputs and stores what it produced:
+
+* e2e_reference_test.npz -- the end-to-end cases of the reference GPU test
+  (test/test_frsz_gpu.cu:382-410): the 11 (bits, E, T) combinations over the
+  repeating pattern, n = 2049 (fp64) and 2160 (fp32), compressed into a 0xFF
+  canary buffer with 128 bytes of slack (:332-335); full bytes stored.
+* back_and_forth32.npz -- the E=1, 32-bit lossless case (:422-441) with a
+  fixed seed instead of std::random_device, 4096 values.
+* digests.json -- SHA-256 of the compressed buffer and of the decompressed
+  values for seeded random cases over bits 4..64, block sizes
+  {1, 2, 4, 5, 8, 16, 32, 64, 128, 256, 512, 1024} and both float types, plus
+  the 2^20-element fp64 N(0,1) E32/b32 round trip.
+
+Usage: python tests/golden/make_golden.py   (needs oracle/_ref built)
+"""
+from __future__ import annotations
+
+import hashlib
+import json
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+
+import oracle  # noqa: E402
+from frsz_b200 import workloads  # noqa: E402
+
+E2E_F64 = [(32, 32), (16, 32), (16, 8), (15, 8), (9, 8), (9, 4), (9, 5)]
+E2E_F32 = [(16, 8), (15, 8), (9, 4), (9, 5)]
+BLOCKS = [1, 2, 4, 5, 8, 16, 32, 64, 128, 256, 512, 1024]
+
+
+def sha(a: np.ndarray) -> str:
+    return hashlib.sha256(np.ascontiguousarray(a).view(np.uint8).tobytes()).hexdigest()
+
+
+def random_case_input(dtype, bits: int, E: int, n: int, seed: int) -> np.ndarray:
+    """Input of one digest case: alternates N(0,1), log-uniform magnitudes
+    and the reference pattern by seed; fp64 at bits <= 8 stays within
+    |x| < 2^127 (larger values wrap the int8 exponent into undefined shifts)."""
+    kind = seed % 3
+    if kind == 0:
+        x = workloads.normal_np(n, dtype, seed)
+    elif kind == 1:
+        if dtype == np.float64 and bits <= 8:
+            x = workloads.loguniform_np(n, dtype, seed, lo=-30, hi=30)
+        elif dtype == np.float64:
+            x = workloads.loguniform_np(n, dtype, seed, lo=-300, hi=300)
+        else:
+            x = workloads.loguniform_np(n, dtype, seed, lo=-40, hi=38)
+    else:
+        x = workloads.reference_pattern(n, dtype)
+    return x
+
+
+def digest_cases():
+    cases = []
+    seed = 1000
+    for dtype in (np.float32, np.float64):
+        max_bits = 32 if dtype == np.float32 else 64
+        for bits in range(4, max_bits + 1):
+            for E in BLOCKS:
+                n = [1, 31, 33, 777, 2049][seed % 5]
+                cases.append({"dtype": np.dtype(dtype).name, "bits": bits, "E": E, "n": n, "seed": seed})
+                seed += 1
+    return cases
+
+
+def main() -> None:
+    if not oracle.ref_available():
+        oracle.build(with_reference=True)
+    # ---- reference GPU-test end-to-end cases
+    e2e = {}
+    for dtype, combos, n in ((np.float64, E2E_F64, 2049), (np.float32, E2E_F32, 2160)):
+        x = workloads.reference_pattern(n, dtype)
+        for bits, E in combos:
+            size = oracle.compressed_bytes(bits, E, n) + 128
+            buf = np.full(size, 0xFF, dtype=np.uint8)
+            oracle.ref_compress_into(x, buf, bits, E)
+            e2e[f"{np.dtype(dtype).name}_b{bits}_e{E}"] = buf
+    np.savez_compressed(os.path.join(HERE, "e2e_reference_test.npz"), **e2e)
+
+    # ---- E = 1, 32-bit lossless
+    x = workloads.uniform_np(4096, -1e8, 1e8, np.float32, seed=7)
+    buf = np.full(oracle.compressed_bytes(32, 1, x.size) + 128, 0xFF, dtype=np.uint8)
+    oracle.ref_compress_into(x, buf, 32, 1)
+    np.savez_compressed(os.path.join(HERE, "back_and_forth32.npz"), input=x, compressed=buf)
+
+    # ---- digests
+    out = {"cases": []}
+    for c in digest_cases():
+        dt = np.dtype(c["dtype"]).type
+        x = random_case_input(dt, c["bits"], c["E"], c["n"], c["seed"])
+        comp = oracle.ref_compress(x, c["bits"], c["E"], canary=0xA5)
+        dec = oracle.ref_decompress(comp, c["n"], dt, c["bits"], c["E"])
+        out["cases"].append({**c, "compressed_sha256": sha(comp), "decompressed_sha256": sha(dec),
+                             "compressed_bytes": int(comp.size)})
+    x = workloads.normal_np(1 << 20, np.float64, 42)
+    comp = oracle.ref_compress(x, 32, 32, canary=0xFF)
+    dec = oracle.ref_decompress(comp, x.size, np.float64, 32, 32)
+    out["config1"] = {"dtype": "float64", "n": 1 << 20, "bits": 32, "E": 32, "seed": 42, "canary": 255,
+                      "compressed_sha256": sha(comp), "decompressed_sha256": sha(dec),
+                      "compressed_bytes": int(comp.size)}
+    with open(os.path.join(HERE, "digests.json"), "w") as f:
+        json.dump(out, f, indent=1)
+    print("wrote fixtures to", HERE)
+
+
+if __name__ == "__main__":
+    main()
