@@ -17,8 +17,10 @@ LIB = os.path.join(HERE, "libfrsz2_b200.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-shared", "--expt-relaxed-constexpr"]
 
-# translation units of the library (headers are tracked for staleness only)
-SOURCES = ["frsz2_capi.cu"]
+# translation units of the library (headers are tracked for staleness only);
+# compiled in parallel, then linked
+SOURCES = ["frsz2_capi.cu", "frsz2_fast_f32.cu", "frsz2_fast_f64.cu"]
+OBJDIR = os.path.join(HERE, "_build")
 
 
 def _sources():
@@ -46,11 +48,24 @@ def nvcc() -> str:
 def build(force: bool = False, verbose: bool = False) -> str:
     if not force and not stale():
         return LIB
-    cmd = [nvcc(), *ARCH, *NVCC_FLAGS, "-I", os.path.join(ROOT, "include"), "-o", LIB, *_sources()]
-    if verbose:
-        cmd.insert(1, "-Xptxas=-v")
-        print(" ".join(cmd), flush=True)
-    subprocess.run(cmd, check=True)
+    os.makedirs(OBJDIR, exist_ok=True)
+    inc = ["-I", os.path.join(ROOT, "include")]
+    flags = [f for f in NVCC_FLAGS if f != "-shared"]
+    procs, objs = [], []
+    for src in _sources():
+        obj = os.path.join(OBJDIR, os.path.basename(src).replace(".cu", ".o"))
+        cmd = [nvcc(), *ARCH, *flags, *inc, "-c", src, "-o", obj]
+        if verbose:
+            cmd.insert(1, "-Xptxas=-v")
+            print(" ".join(cmd), flush=True)
+        procs.append((subprocess.Popen(cmd), cmd))
+        objs.append(obj)
+    for p, cmd in procs:
+        if p.wait() != 0:
+            raise subprocess.CalledProcessError(p.returncode, cmd)
+    tmp = LIB + ".tmp"
+    subprocess.run([nvcc(), *ARCH, "-shared", "-o", tmp, *objs], check=True)
+    os.replace(tmp, LIB)
     return LIB
 
 

@@ -1,5 +1,6 @@
 // frsz2_capi.cu -- C ABI of libfrsz2_b200.so: argument checks, kernel choice,
 // launch geometry, and the host-buffer path with pipelined copies.
+#include "frsz2_fast_dispatch.hpp"
 #include "frsz2_kernels.cuh"
 #include "frsz2_launch.hpp"
 
@@ -114,10 +115,26 @@ static unsigned grid_for(std::uint64_t work_items, std::uint64_t per_cta)
   return (unsigned)std::max<std::uint64_t>(1, std::min(need, cap));
 }
 
+// Compile-time-width kernels when an instance and the layout allow it;
+// cudaErrorNotSupported means "use the runtime-width kernels".
+template<class T>
+static cudaError_t try_fast(bool compress, const Job& j, cudaStream_t s)
+{
+  const void* values = compress ? j.values_in : j.values_out;
+  if (!fast_eligible(j, sizeof(T) == 8, values, j.words)) return cudaErrorNotSupported;
+  const unsigned grid = (unsigned)std::min<std::uint64_t>(j.tiles, 1u << 30);
+  return sizeof(T) == 8 ? launch_fast_f64(j.bits, compress, j, s, grid) : launch_fast_f32(j.bits, compress, j, s, grid);
+}
+
 template<class T>
 static int launch_compress_t(const Job& j, int dtype, cudaStream_t s, bool* used_tile)
 {
   if (j.n == 0) return FRSZ2_OK;
+  const cudaError_t fe = try_fast<T>(true, j, s);
+  if (fe != cudaErrorNotSupported) {
+    if (used_tile) *used_tile = true;
+    return cuda_status(fe, "compress launch");
+  }
   const bool tile = tile_eligible(j, dtype, j.values_in, j.words);
   if (used_tile) *used_tile = tile;
   if (tile) {
@@ -137,6 +154,11 @@ template<class T>
 static int launch_decompress_t(const Job& j, int dtype, cudaStream_t s, bool* used_tile)
 {
   if (j.n == 0) return FRSZ2_OK;
+  const cudaError_t fe = try_fast<T>(false, j, s);
+  if (fe != cudaErrorNotSupported) {
+    if (used_tile) *used_tile = true;
+    return cuda_status(fe, "decompress launch");
+  }
   const bool tile = tile_eligible(j, dtype, j.values_out, j.words);
   if (used_tile) *used_tile = tile;
   if (tile) {
@@ -281,7 +303,7 @@ int host_codec(bool compress, int dtype, int bits, int E, const void* h_in, std:
       (nbk - 1) * (std::uint64_t)L.block_bytes +
       (last ? written_block_bytes(last_cnt, bits, L.W) : L.block_bytes);
     if (compress) {
-      Job j = job_for_slice(L, dtype, b0, nbk, static_cast<std::uint8_t*>(S.d_values) + e0 * es, nullptr, d_buf);
+      Job j = job_for_slice(L, dtype, b0, nbk, S.d_values, nullptr, d_buf);
       if ((rc = cuda_status(cudaMemcpyAsync(static_cast<std::uint8_t*>(S.d_values) + e0 * es, hb_in + e0 * es,
                                             ne * es, cudaMemcpyHostToDevice, s),
                             "H2D")))
@@ -293,7 +315,7 @@ int host_codec(bool compress, int dtype, int bits, int E, const void* h_in, std:
       if ((rc = cuda_status(cudaMemcpyAsync(hb_out + w_off, d_buf + w_off, w_len, cudaMemcpyDeviceToHost, s), "D2H")))
         return rc;
     } else {
-      Job j = job_for_slice(L, dtype, b0, nbk, nullptr, static_cast<std::uint8_t*>(S.d_values) + e0 * es, d_buf);
+      Job j = job_for_slice(L, dtype, b0, nbk, nullptr, S.d_values, d_buf);
       if ((rc = cuda_status(cudaMemcpyAsync(d_buf + exp_off, hb_in + exp_off, exp_len, cudaMemcpyHostToDevice, s),
                             "H2D")))
         return rc;

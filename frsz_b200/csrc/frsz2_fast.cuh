@@ -1,0 +1,582 @@
+// frsz2_fast.cuh -- compile-time-width FRSZ2 kernels (the hot path).
+//
+// One kernel instance per (float type, bits).  Lane mapping: each lane owns a
+// contiguous run of P = 32 / sizeof(T) values (one 256-bit load / store), so
+// its packed codes form one contiguous segment of L = P * bits stream bits;
+// packing and unpacking are constant shifts, plus one neighbour shuffle when
+// L is not a multiple of 32.  A warp row is 32 * P values; a 256-thread CTA
+// handles a tile of 2 rows per warp (4096 fp32 / 2048 fp64 values).
+//
+// Arithmetic.  For blocks whose exponent lies in the "plain" domain (no
+// Inf/NaN, e_b >= -95 for fp32 / >= -959 for fp64, no int8 exponent wrap)
+// the reference's integer align-and-truncate (floating_to_fixed +
+// uint_fp_to_compressed, include/frsz2.hpp:352-376, 555-558) equals
+//     code = trunc(|x| * 2^(bits-2-e_b)) | sign << (bits-1)
+// because scaling by a power of two is exact there, subnormal inputs
+// truncate to 0 on both sides, and the code fits in bits-1 bits.  Likewise
+// fixed_to_floating (include/frsz2.hpp:378-399) equals
+//     x_hat = rz_convert(mag) * 2^(e_b-bits+2)   (mag != 0)
+//     x_hat = 2^(e_b-31)                          (mag == 0, the clz quirk)
+// with the sign or-ed in: rounding toward zero keeps the same 24 / 53 leading
+// bits the reference's shift keeps, and every result is a normal number.
+// Blocks outside the plain domain use the exact integer path of
+// frsz2_common.cuh (a block-uniform branch), so results are bit-exact for
+// every input.
+#pragma once
+
+#include "frsz2_kernels.cuh"
+
+#include <type_traits>
+
+namespace frsz2b {
+
+template<class T, int BITS>
+struct fast_cfg
+{
+  using U = typename fp<T>::U;
+  using C = std::conditional_t<(BITS <= 32), std::uint32_t, std::uint64_t>;
+  static constexpr int P = 32 / (int)sizeof(T);  // values per lane
+  static constexpr int L = P * BITS;             // segment bits per lane
+  static constexpr int NW = (L + 31) / 32;       // segment words
+  static constexpr bool ALIGNED = (L % 32) == 0; // segments start on word boundaries
+  static constexpr int ROW = 32 * P;             // values per warp row
+  static constexpr int RPW = 2;                  // rows per warp per tile
+  static constexpr int WARPS = kNT / 32;
+  static constexpr int ROWS = WARPS * RPW;       // rows per tile
+  static constexpr int TE = ROWS * ROW;          // values per tile
+  static constexpr int W = BITS <= 8 ? 8 : BITS <= 16 ? 16 : BITS <= 32 ? 32 : 64;
+};
+
+// ---------------------------------------------------------------- PTX helpers
+
+__device__ __forceinline__ void ld256_stream(const void* p, std::uint32_t (&v)[8])
+{
+  asm volatile("ld.global.nc.L1::no_allocate.v8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+               : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7])
+               : "l"(p));
+}
+
+__device__ __forceinline__ void st256_stream(void* p, const std::uint32_t (&v)[8])
+{
+  asm volatile("st.global.cs.v8.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};" ::"l"(p), "r"(v[0]), "r"(v[1]), "r"(v[2]),
+               "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7])
+               : "memory");
+}
+
+// N consecutive 32-bit words at p, p aligned to 4 * (largest power of two
+// dividing N), at most 32 bytes.
+template<int N>
+__device__ __forceinline__ void load_words(const std::uint32_t* p, std::uint32_t (&w)[N])
+{
+  constexpr int V = (N % 8 == 0) ? 8 : (N % 4 == 0) ? 4 : (N % 2 == 0) ? 2 : 1;
+#pragma unroll
+  for (int i = 0; i < N; i += V) {
+    if constexpr (V == 8) {
+      std::uint32_t t[8];
+      asm volatile("ld.global.nc.L1::no_allocate.v8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                   : "=r"(t[0]), "=r"(t[1]), "=r"(t[2]), "=r"(t[3]), "=r"(t[4]), "=r"(t[5]), "=r"(t[6]), "=r"(t[7])
+                   : "l"(p + i));
+#pragma unroll
+      for (int k = 0; k < 8; ++k) w[i + k] = t[k];
+    } else if constexpr (V == 4) {
+      const uint4 t = __ldg(reinterpret_cast<const uint4*>(p + i));
+      w[i] = t.x;
+      w[i + 1] = t.y;
+      w[i + 2] = t.z;
+      w[i + 3] = t.w;
+    } else if constexpr (V == 2) {
+      const uint2 t = __ldg(reinterpret_cast<const uint2*>(p + i));
+      w[i] = t.x;
+      w[i + 1] = t.y;
+    } else {
+      w[i] = __ldg(p + i);
+    }
+  }
+}
+
+template<int N>
+__device__ __forceinline__ void store_words(std::uint32_t* p, const std::uint32_t (&w)[N])
+{
+  constexpr int V = (N % 8 == 0) ? 8 : (N % 4 == 0) ? 4 : (N % 2 == 0) ? 2 : 1;
+#pragma unroll
+  for (int i = 0; i < N; i += V) {
+    if constexpr (V == 8) {
+      std::uint32_t t[8];
+#pragma unroll
+      for (int k = 0; k < 8; ++k) t[k] = w[i + k];
+      st256_stream(p + i, t);
+    } else if constexpr (V == 4) {
+      __stcs(reinterpret_cast<uint4*>(p + i), make_uint4(w[i], w[i + 1], w[i + 2], w[i + 3]));
+    } else if constexpr (V == 2) {
+      __stcs(reinterpret_cast<uint2*>(p + i), make_uint2(w[i], w[i + 1]));
+    } else {
+      __stcs(reinterpret_cast<unsigned int*>(p + i), w[i]);
+    }
+  }
+}
+
+// Store one 32-bit stream word at tile byte offset `off`, keeping bytes at or
+// beyond `limit` untouched (the unwritten tail of a partial last block).
+__device__ __forceinline__ void store_word_bounded(std::uint8_t* base, std::uint32_t off, std::uint32_t limit,
+                                                   std::uint32_t v)
+{
+  if (off + 4u <= limit) {
+    *reinterpret_cast<std::uint32_t*>(base + off) = v;
+  } else {
+    for (std::uint32_t q = 0; off + q < limit; ++q) base[off + q] = (std::uint8_t)(v >> (8 * q));
+  }
+}
+
+// ---------------------------------------------------------------- bit fields
+
+// Insert the low NB bits of v (zero above NB) at stream bit POS of seg.
+template<int POS, int NB, int N, class V>
+__device__ __forceinline__ void put_bits(std::uint32_t (&seg)[N], V v)
+{
+  constexpr int q = POS / 32, r = POS % 32;
+  if constexpr (sizeof(V) == 4) {
+    seg[q] |= v << r;
+    if constexpr (r != 0 && r + NB > 32) seg[q + 1] |= v >> (32 - r);
+  } else {
+    seg[q] |= (std::uint32_t)(v << r);
+    if constexpr (r + NB > 32) seg[q + 1] |= (std::uint32_t)(r == 0 ? (v >> 32) : (v >> (32 - r)));
+    if constexpr (r + NB > 64) seg[q + 2] |= (std::uint32_t)(v >> (64 - r));
+  }
+}
+
+// NB-bit field at stream bit POS of seg.
+template<int POS, int NB, int N>
+__device__ __forceinline__ auto get_bits(const std::uint32_t (&seg)[N])
+{
+  constexpr int q = POS / 32, r = POS % 32;
+  if constexpr (NB <= 32) {
+    constexpr std::uint32_t mask = NB == 32 ? 0xFFFFFFFFu : ((1u << NB) - 1u);
+    if constexpr (r + NB <= 32)
+      return (seg[q] >> r) & mask;
+    else
+      return __funnelshift_r(seg[q], seg[q + 1], r) & mask;
+  } else {
+    constexpr std::uint64_t mask = NB == 64 ? ~0ull : ((1ull << NB) - 1ull);
+    const std::uint32_t lo = r == 0 ? seg[q] : __funnelshift_r(seg[q], seg[q + 1], r);
+    std::uint32_t hi;
+    if constexpr (r == 0)
+      hi = seg[q + 1];
+    else if constexpr (r + NB > 64)
+      hi = __funnelshift_r(seg[q + 1], seg[q + 2], r);
+    else
+      hi = seg[q + 1] >> r;
+    return ((((std::uint64_t)hi) << 32) | lo) & mask;
+  }
+}
+
+template<int K, int BITS, int N, class C, int P>
+__device__ __forceinline__ void pack_all(std::uint32_t (&seg)[N], const C (&c)[P])
+{
+  if constexpr (K < P) {
+    put_bits<K * BITS, BITS>(seg, c[K]);
+    pack_all<K + 1, BITS>(seg, c);
+  }
+}
+
+template<int K, int BITS, int N, class C, int P>
+__device__ __forceinline__ void unpack_all(const std::uint32_t (&seg)[N], C (&c)[P])
+{
+  if constexpr (K < P) {
+    c[K] = (C)get_bits<K * BITS, BITS>(seg);
+    unpack_all<K + 1, BITS>(seg, c);
+  }
+}
+
+// ---------------------------------------------------------------- keys
+
+// Block-max key of a value: the magnitude bits that decide the exponent
+// field (all of |x| for fp32, the high word of |x| for fp64).  A key at or
+// above KEY_SPECIAL means the block holds +-Inf or NaN.
+template<class T>
+struct key_of;
+template<>
+struct key_of<float>
+{
+  static constexpr std::uint32_t SPECIAL = 0x7F800000u;
+  static constexpr int FSHIFT = 23;
+  __device__ static std::uint32_t raw(std::uint32_t u) { return u & 0x7FFFFFFFu; }
+  __device__ static std::uint32_t clean(std::uint32_t u)
+  {
+    const std::uint32_t a = u & 0x7FFFFFFFu;
+    return a > 0x7F800000u ? 0u : a;
+  }
+};
+template<>
+struct key_of<double>
+{
+  static constexpr std::uint32_t SPECIAL = 0x7FF00000u;
+  static constexpr int FSHIFT = 20;
+  __device__ static std::uint32_t raw(std::uint64_t u) { return (std::uint32_t)(u >> 32) & 0x7FFFFFFFu; }
+  __device__ static std::uint32_t clean(std::uint64_t u)
+  {
+    const std::uint64_t a = u & 0x7FFFFFFFFFFFFFFFull;
+    return a > 0x7FF0000000000000ull ? 0u : (std::uint32_t)(a >> 32);
+  }
+};
+
+// Exponent range in which the float-arithmetic formulas are exact.
+template<class T>
+__device__ __forceinline__ bool plain_exponent(std::int64_t be)
+{
+  if constexpr (sizeof(T) == 4)
+    return be >= -95 && be <= 127;
+  else
+    return be >= -959 && be <= 1023;
+}
+
+template<class T>
+__device__ __forceinline__ T pow2(int e) // 2^e, e within the normal range
+{
+  if constexpr (sizeof(T) == 4)
+    return __uint_as_float((std::uint32_t)(e + 127) << 23);
+  else
+    return __longlong_as_double((long long)(e + 1023) << 52);
+}
+
+// ---------------------------------------------------------------- encode / decode
+
+template<class T, int BITS>
+__device__ __forceinline__ typename fast_cfg<T, BITS>::C encode_plain(typename fp<T>::U u, T scale)
+{
+  using Cfg = fast_cfg<T, BITS>;
+  using C = typename Cfg::C;
+  const T x = from_bits<T>(u);
+  if constexpr (sizeof(T) == 4) {
+    const std::uint32_t mag = __float2uint_rz(fabsf(x) * scale);
+    return mag | ((u >> (32 - BITS)) & (1u << (BITS - 1)));
+  } else {
+    const std::uint32_t hi = (std::uint32_t)(u >> 32);
+    if constexpr (BITS <= 32) {
+      const std::uint32_t mag = __double2uint_rz(fabs(x) * scale);
+      return mag | ((hi >> (32 - BITS)) & (1u << (BITS - 1)));
+    } else {
+      const std::uint64_t mag = __double2ull_rz(fabs(x) * scale);
+      return (C)(mag | ((std::uint64_t)(hi >> 31) << (BITS - 1)));
+    }
+  }
+}
+
+template<class T, int BITS>
+__device__ __forceinline__ typename fp<T>::U decode_plain(typename fast_cfg<T, BITS>::C code, T inv,
+                                                          typename fp<T>::U zero_bits)
+{
+  using U = typename fp<T>::U;
+  using C = typename fast_cfg<T, BITS>::C;
+  constexpr C MAGMASK = (C(1) << (BITS - 1)) - 1;
+  const C mag = code & MAGMASK;
+  U r;
+  if constexpr (sizeof(T) == 4) {
+    r = __float_as_uint(__uint2float_rz(mag) * inv);
+  } else if constexpr (BITS <= 32) {
+    r = (U)__double_as_longlong(__uint2double_rn(mag) * inv);
+  } else {
+    r = (U)__double_as_longlong(__ull2double_rz(mag) * inv);
+  }
+  r = mag == 0 ? zero_bits : r;
+  return r | ((U)(code >> (BITS - 1)) << (fp<T>::UBITS - 1));
+}
+
+// ---------------------------------------------------------------- compress
+
+template<class T, int BITS>
+__global__ void __launch_bounds__(kNT) k_compress_fast(Job j)
+{
+  using Cfg = fast_cfg<T, BITS>;
+  using U = typename Cfg::U;
+  using C = typename Cfg::C;
+  using K = key_of<T>;
+  constexpr int P = Cfg::P, L = Cfg::L, NW = Cfg::NW, ROW = Cfg::ROW, RPW = Cfg::RPW, TE = Cfg::TE,
+                W = Cfg::W;
+  __shared__ std::uint32_t s_rmax[2][Cfg::ROWS];
+
+  const T* __restrict__ x = static_cast<const T*>(j.values_in);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int E = j.E, log2E = j.log2E;
+  const int G = E / P; // lanes per exponent block
+  const int TB = (int)j.tile_blocks;
+
+  for (std::uint64_t tile = blockIdx.x; tile < j.tiles; tile += gridDim.x) {
+    const std::uint64_t e0 = tile * (std::uint64_t)TE;
+    const std::uint64_t rem64 = j.n - e0;
+    const bool full = rem64 >= (std::uint64_t)TE;
+    const int rem = full ? TE : (int)rem64;
+    const int nbt = full ? TB : ((rem + E - 1) >> log2E);
+    const std::uint64_t b0 = tile * (std::uint64_t)TB;
+
+    U u[RPW][P];
+#pragma unroll
+    for (int rr = 0; rr < RPW; ++rr) {
+      const int idx = (rr * Cfg::WARPS + warp) * ROW + lane * P;
+      if (full || idx + P <= rem) {
+        std::uint32_t v[8];
+        ld256_stream(x + e0 + idx, v);
+#pragma unroll
+        for (int i = 0; i < P; ++i) {
+          if constexpr (sizeof(T) == 4)
+            u[rr][i] = v[i];
+          else
+            u[rr][i] = ((std::uint64_t)v[2 * i + 1] << 32) | v[2 * i];
+        }
+      } else {
+#pragma unroll
+        for (int i = 0; i < P; ++i) u[rr][i] = (idx + i < rem) ? to_bits<T>(x[e0 + idx + i]) : U(0);
+      }
+    }
+
+    // block maxima: raw keys detect Inf/NaN, clean keys skip NaN like std::max
+    std::uint32_t km[RPW], kc[RPW];
+    bool any_special = false;
+#pragma unroll
+    for (int rr = 0; rr < RPW; ++rr) {
+      std::uint32_t m = K::raw(u[rr][0]);
+#pragma unroll
+      for (int i = 1; i < P; ++i) m = max(m, K::raw(u[rr][i]));
+      km[rr] = m;
+      any_special |= m >= K::SPECIAL;
+    }
+    const bool warp_special = __any_sync(0xFFFFFFFFu, any_special);
+#pragma unroll
+    for (int rr = 0; rr < RPW; ++rr) {
+      if (warp_special) {
+        std::uint32_t m = K::clean(u[rr][0]);
+#pragma unroll
+        for (int i = 1; i < P; ++i) m = max(m, K::clean(u[rr][i]));
+        kc[rr] = m;
+      } else {
+        kc[rr] = km[rr];
+      }
+    }
+    if (G <= 32) {
+      for (int s = 1; s < G; s <<= 1) {
+#pragma unroll
+        for (int rr = 0; rr < RPW; ++rr) km[rr] = max(km[rr], __shfl_xor_sync(0xFFFFFFFFu, km[rr], s));
+        if (warp_special) {
+#pragma unroll
+          for (int rr = 0; rr < RPW; ++rr) kc[rr] = max(kc[rr], __shfl_xor_sync(0xFFFFFFFFu, kc[rr], s));
+        }
+      }
+      if (!warp_special) {
+#pragma unroll
+        for (int rr = 0; rr < RPW; ++rr) kc[rr] = km[rr];
+      }
+    } else {
+      // an exponent block spans G/32 whole rows of this tile
+#pragma unroll
+      for (int rr = 0; rr < RPW; ++rr) {
+        const std::uint32_t a = __reduce_max_sync(0xFFFFFFFFu, km[rr]);
+        const std::uint32_t b = __reduce_max_sync(0xFFFFFFFFu, kc[rr]);
+        if (lane == 0) {
+          s_rmax[0][rr * Cfg::WARPS + warp] = a;
+          s_rmax[1][rr * Cfg::WARPS + warp] = b;
+        }
+      }
+      __syncthreads();
+      const int rpb = G / 32;
+#pragma unroll
+      for (int rr = 0; rr < RPW; ++rr) {
+        const int row0 = ((rr * Cfg::WARPS + warp) / rpb) * rpb;
+        std::uint32_t a = 0, b = 0;
+        for (int q = 0; q < rpb; ++q) {
+          a = max(a, s_rmax[0][row0 + q]);
+          b = max(b, s_rmax[1][row0 + q]);
+        }
+        km[rr] = a;
+        kc[rr] = b;
+      }
+      __syncthreads();
+    }
+
+    const int last_cnt = rem - (nbt - 1) * E;
+    const std::uint32_t wb = full ? (std::uint32_t)TB * j.block_bytes
+                                  : (std::uint32_t)(nbt - 1) * j.block_bytes + written_block_bytes(last_cnt, BITS, W);
+    std::uint8_t* __restrict__ dst = j.words + b0 * (std::uint64_t)j.block_bytes;
+
+#pragma unroll
+    for (int rr = 0; rr < RPW; ++rr) {
+      const int row = rr * Cfg::WARPS + warp;
+      const int idx = row * ROW + lane * P;
+      const int bl = idx >> log2E;
+      const int field = (int)(kc[rr] >> K::FSHIFT);
+      const std::int64_t ex = exponent_of_field<T>(field);
+      const std::int64_t be = wrap_signed(ex, W);
+      const bool plain = km[rr] < K::SPECIAL && be == ex && plain_exponent<T>(be);
+
+      C c[P];
+      if (plain) {
+        const T scale = pow2<T>(BITS - 2 - (int)be);
+#pragma unroll
+        for (int i = 0; i < P; ++i) c[i] = encode_plain<T, BITS>(u[rr][i], scale);
+      } else {
+#pragma unroll
+        for (int i = 0; i < P; ++i) c[i] = (C)to_code<T>(u[rr][i], (std::int16_t)be, BITS);
+      }
+      if ((idx & (E - 1)) == 0 && bl < nbt)
+        store_word(j.exps + (b0 + (std::uint64_t)bl) * (std::uint64_t)(W / 8), (std::uint64_t)be, W);
+
+      std::uint32_t seg[NW + 1];
+#pragma unroll
+      for (int i = 0; i <= NW; ++i) seg[i] = 0;
+      pack_all<0, BITS>(seg, c);
+
+      // stream bits of this row start at row * ROW * BITS (a word boundary)
+      const std::uint32_t row_byte = (std::uint32_t)row * (std::uint32_t)(ROW * BITS / 8);
+      if constexpr (Cfg::ALIGNED) {
+        const std::uint32_t off = row_byte + (std::uint32_t)lane * (std::uint32_t)(L / 8);
+        std::uint32_t out[NW];
+#pragma unroll
+        for (int i = 0; i < NW; ++i) out[i] = seg[i];
+        if (full || off + 4u * NW <= wb) {
+          store_words<NW>(reinterpret_cast<std::uint32_t*>(dst + off), out);
+        } else {
+#pragma unroll
+          for (int i = 0; i < NW; ++i)
+            if (off + 4u * i < wb) store_word_bounded(dst, off + 4u * i, wb, out[i]);
+        }
+      } else {
+        // words whose first bit lies in this lane's segment; the tail of the
+        // last one comes from the next lane's first word
+        const std::uint32_t h0 = __shfl_down_sync(0xFFFFFFFFu, seg[0], 1);
+        constexpr int q = L / 32, r = L % 32;
+        seg[q] |= h0 << r;
+        seg[q + 1] = h0 >> (32 - r);
+        const std::uint32_t S = (std::uint32_t)lane * L;
+        const std::uint32_t f = (S + 31u) >> 5;
+        const int d = (int)(f * 32u - S);
+        const int k = (int)(((S + L + 31u) >> 5) - f);
+#pragma unroll
+        for (int i = 0; i < NW; ++i) {
+          if (i < k) {
+            const std::uint32_t w = __funnelshift_r(seg[i], seg[i + 1], d);
+            const std::uint32_t off = row_byte + 4u * (f + (std::uint32_t)i);
+            if (full)
+              __stcs(reinterpret_cast<unsigned int*>(dst + off), w);
+            else if (off < wb)
+              store_word_bounded(dst, off, wb, w);
+          }
+        }
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------- decompress
+
+template<class T, int BITS>
+__global__ void __launch_bounds__(kNT) k_decompress_fast(Job j)
+{
+  using Cfg = fast_cfg<T, BITS>;
+  using U = typename Cfg::U;
+  using C = typename Cfg::C;
+  constexpr int P = Cfg::P, L = Cfg::L, NW = Cfg::NW, ROW = Cfg::ROW, RPW = Cfg::RPW, TE = Cfg::TE,
+                W = Cfg::W;
+
+  T* __restrict__ y = static_cast<T*>(j.values_out);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int log2E = j.log2E;
+  const int TB = (int)j.tile_blocks;
+
+  for (std::uint64_t tile = blockIdx.x; tile < j.tiles; tile += gridDim.x) {
+    const std::uint64_t e0 = tile * (std::uint64_t)TE;
+    const std::uint64_t rem64 = j.n - e0;
+    const bool full = rem64 >= (std::uint64_t)TE;
+    const int rem = full ? TE : (int)rem64;
+    const std::uint64_t b0 = tile * (std::uint64_t)TB;
+    const std::uint32_t* __restrict__ src =
+      reinterpret_cast<const std::uint32_t*>(j.words + b0 * (std::uint64_t)j.block_bytes);
+
+    std::uint32_t wv[RPW][NW + 1];
+    std::int64_t be[RPW];
+#pragma unroll
+    for (int rr = 0; rr < RPW; ++rr) {
+      const int row = rr * Cfg::WARPS + warp;
+      const int idx = row * ROW + lane * P;
+      if (!full && idx >= rem) continue;
+      be[rr] = load_exp(j.exps + (b0 + (std::uint64_t)(idx >> log2E)) * (std::uint64_t)(W / 8), W);
+      const std::uint32_t S = (std::uint32_t)idx * BITS; // tile stream bit
+      if constexpr (Cfg::ALIGNED) {
+        std::uint32_t t[NW];
+        load_words<NW>(src + (S >> 5), t);
+#pragma unroll
+        for (int i = 0; i < NW; ++i) wv[rr][i] = t[i];
+        wv[rr][NW] = 0;
+      } else {
+        const std::uint32_t w0 = S >> 5;
+        const int o = (int)(S & 31u);
+#pragma unroll
+        for (int i = 0; i < NW; ++i) wv[rr][i] = __ldg(src + w0 + i);
+        // the extra word only when the segment reaches into it
+        wv[rr][NW] = (o + L > 32 * NW) ? __ldg(src + w0 + NW) : 0u;
+      }
+    }
+
+#pragma unroll
+    for (int rr = 0; rr < RPW; ++rr) {
+      const int row = rr * Cfg::WARPS + warp;
+      const int idx = row * ROW + lane * P;
+      if (!full && idx >= rem) continue;
+      std::uint32_t seg[NW + 1];
+      if constexpr (Cfg::ALIGNED) {
+#pragma unroll
+        for (int i = 0; i <= NW; ++i) seg[i] = wv[rr][i];
+      } else {
+        const int o = (int)(((std::uint32_t)idx * BITS) & 31u);
+#pragma unroll
+        for (int i = 0; i < NW; ++i) seg[i] = __funnelshift_r(wv[rr][i], wv[rr][i + 1], o);
+        seg[NW] = 0;
+      }
+      C c[P];
+      unpack_all<0, BITS>(seg, c);
+
+      U outb[P];
+      const std::int64_t b = be[rr];
+      if (plain_exponent<T>(b)) {
+        const T inv = pow2<T>((int)b - BITS + 2);
+        const U zero_bits = sizeof(T) == 4 ? (U)((std::uint32_t)(b + 96) << 23)
+                                           : (U)((std::uint64_t)(b + 992) << 52);
+#pragma unroll
+        for (int i = 0; i < P; ++i) outb[i] = decode_plain<T, BITS>(c[i], inv, zero_bits);
+      } else {
+#pragma unroll
+        for (int i = 0; i < P; ++i) outb[i] = to_bits<T>(from_code<T>((U)c[i], b, BITS));
+      }
+
+      if (full || idx + P <= rem) {
+        std::uint32_t v[8];
+#pragma unroll
+        for (int i = 0; i < P; ++i) {
+          if constexpr (sizeof(T) == 4) {
+            v[i] = outb[i];
+          } else {
+            v[2 * i] = (std::uint32_t)outb[i];
+            v[2 * i + 1] = (std::uint32_t)(outb[i] >> 32);
+          }
+        }
+        st256_stream(y + e0 + idx, v);
+      } else {
+        for (int i = 0; i < P && idx + i < rem; ++i) y[e0 + idx + i] = from_bits<T>(outb[i]);
+      }
+    }
+  }
+}
+
+// Requirements of the fast kernels for (dtype, bits, E) and pointers, beyond
+// having an instance for `bits`.
+__host__ inline bool fast_eligible(const Job& j, int dtype_is_f64, const void* values, const void* words)
+{
+  const int P = dtype_is_f64 ? 4 : 8;
+  const int TE = dtype_is_f64 ? 2048 : 4096;
+  const int E = j.E;
+  if (E < P || E > TE || (E & (E - 1)) != 0) return false;
+  if (((std::uint64_t)E * (std::uint64_t)j.bits) % (std::uint64_t)j.W != 0) return false; // no block pad
+  if (dtype_is_f64 && j.bits < 8) return false;
+  if (reinterpret_cast<std::uintptr_t>(values) % 32 != 0) return false;
+  if (reinterpret_cast<std::uintptr_t>(words) % 32 != 0) return false;
+  return true;
+}
+
+} // namespace frsz2b

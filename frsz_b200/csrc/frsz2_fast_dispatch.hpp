@@ -1,0 +1,42 @@
+// frsz2_fast_dispatch.hpp -- per-width launch table of the fast kernels.
+#pragma once
+
+#include "frsz2_fast.cuh"
+
+#include <array>
+#include <utility>
+
+namespace frsz2b {
+
+// Enqueue the fast compress / decompress kernel for a compile-time width.
+template<class T, int BITS>
+cudaError_t launch_fast_one(bool compress, const Job& j, cudaStream_t s, unsigned grid)
+{
+  if (compress)
+    k_compress_fast<T, BITS><<<grid, kNT, 0, s>>>(j);
+  else
+    k_decompress_fast<T, BITS><<<grid, kNT, 0, s>>>(j);
+  return cudaGetLastError();
+}
+
+using fast_fn = cudaError_t (*)(bool, const Job&, cudaStream_t, unsigned);
+
+template<class T, int LO, int... I>
+constexpr auto make_fast_table(std::integer_sequence<int, I...>)
+{
+  return std::array<fast_fn, sizeof...(I)>{ &launch_fast_one<T, LO + I>... };
+}
+
+// Returns cudaErrorNotSupported when `bits` has no instance.
+#define FRSZ2_FAST_TABLE(T, LO, HI, NAME)                                                                           \
+  cudaError_t NAME(int bits, bool compress, const Job& j, cudaStream_t s, unsigned grid)                          \
+  {                                                                                                                \
+    static constexpr auto table = make_fast_table<T, LO>(std::make_integer_sequence<int, HI - LO + 1>{});          \
+    if (bits < LO || bits > HI) return cudaErrorNotSupported;                                                      \
+    return table[bits - LO](compress, j, s, grid);                                                                 \
+  }
+
+cudaError_t launch_fast_f32(int bits, bool compress, const Job& j, cudaStream_t s, unsigned grid);
+cudaError_t launch_fast_f64(int bits, bool compress, const Job& j, cudaStream_t s, unsigned grid);
+
+} // namespace frsz2b

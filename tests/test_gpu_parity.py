@@ -173,7 +173,10 @@ def test_random_access_elements(cuda, dtype, bits, E):
 
 
 @pytest.mark.parametrize("dtype,bits,E,n", [(np.float32, 16, 32, 1_000_003), (np.float64, 21, 32, 700_001),
-                                            (np.float64, 9, 5, 100_000)])
+                                            (np.float64, 9, 5, 100_000),
+                                            # several 64 MiB pipeline slices, ragged tail
+                                            (np.float32, 12, 32, 40_000_123), (np.float64, 21, 64, 20_000_077),
+                                            (np.float64, 13, 5, 9_000_011)])
 def test_host_buffers(cuda, dtype, bits, E, n):
     """frsz2_compress_host / frsz2_decompress_host: bytes the reference never
     writes keep the caller's canary."""

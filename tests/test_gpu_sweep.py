@@ -1,0 +1,103 @@
+"""GPU parity sweeps over every compile-time width, every block-size path
+and special values (NaN, +-Inf, -0, subnormals, tiny / huge block
+exponents), kernel against the oracle, whole buffers bit-exact."""
+import numpy as np
+import pytest
+import torch
+
+import oracle
+import frsz_b200
+from frsz_b200 import workloads
+
+pytestmark = pytest.mark.gpu
+
+
+def run(x, bits, E, canary=0x6B):
+    size = frsz_b200.compressed_size(x.dtype, bits, E, x.size)
+    buf = torch.full((size,), canary, dtype=torch.uint8, device="cuda")
+    frsz_b200.compress(torch.from_numpy(x).cuda(), bits, E, out=buf)
+    got = buf.cpu().numpy()
+    ref = oracle.compress(x, bits, E, canary=canary)
+    y = frsz_b200.decompress(torch.from_numpy(ref).cuda(), x.size, x.dtype, bits, E).cpu().numpy()
+    yr = oracle.decompress(ref, x.size, x.dtype, bits, E)
+    return got, ref, y, yr
+
+
+def check(x, bits, E):
+    got, ref, y, yr = run(x, bits, E)
+    if not np.array_equal(got, ref):
+        bad = np.nonzero(got != ref)[0]
+        raise AssertionError(f"compressed bytes differ at {bad[:6]} (of {bad.size}); bits={bits} E={E} n={x.size}")
+    if not np.array_equal(y.view(np.uint8), yr.view(np.uint8)):
+        bad = np.nonzero(y.view(np.uint64 if y.dtype == np.float64 else np.uint32) !=
+                         yr.view(np.uint64 if y.dtype == np.float64 else np.uint32))[0]
+        raise AssertionError(f"values differ at {bad[:6]} (of {bad.size}); bits={bits} E={E} n={x.size}")
+
+
+@pytest.mark.parametrize("bits", range(4, 33))
+def test_fp32_every_width(cuda, bits):
+    for E, n in ((32, 3 * 4096 + 77), (8, 4096 + 5), (256, 2 * 4096)):
+        check(workloads.loguniform_np(n, np.float32, seed=bits * 7 + E, lo=-30, hi=30), bits, E)
+
+
+@pytest.mark.parametrize("bits", range(4, 65))
+def test_fp64_every_width(cuda, bits):
+    lo, hi = (-30, 30) if bits <= 8 else (-300, 300)
+    for E, n in ((32, 3 * 2048 + 77), (4, 2048 + 3), (128, 2 * 2048 + 1)):
+        check(workloads.loguniform_np(n, np.float64, seed=bits * 11 + E, lo=lo, hi=hi), bits, E)
+
+
+@pytest.mark.parametrize("dtype,E", [(np.float32, e) for e in (8, 16, 64, 128, 512, 1024, 2048, 4096)] +
+                         [(np.float64, e) for e in (4, 8, 16, 64, 256, 512, 1024, 2048)])
+def test_block_sizes(cuda, dtype, E):
+    for bits in (8, 12, 16, 21, 24, 32) + ((40, 64) if dtype == np.float64 else ()):
+        n = 5 * (4096 if dtype == np.float32 else 2048) + 3 * E // 2 + 1
+        check(workloads.loguniform_np(n, dtype, seed=E + bits, lo=-20, hi=20), bits, E)
+
+
+def special_values(dtype, n, seed):
+    rng = np.random.default_rng(seed)
+    fi = np.finfo(dtype)
+    x = workloads.loguniform_np(n, dtype, seed, lo=-5, hi=5)
+    # whole blocks at the edges of the exponent range
+    B = 64
+    nb = n // B
+    for b in rng.choice(nb, nb // 4, replace=False):
+        kind = rng.integers(5)
+        sl = slice(b * B, (b + 1) * B)
+        if kind == 0:    # tiny: block exponent far below the plain range
+            x[sl] = (rng.standard_normal(B) * float(fi.tiny) * 2 ** rng.integers(0, 40)).astype(dtype)
+        elif kind == 1:  # only subnormals and zeros
+            x[sl] = (rng.random(B) * float(fi.tiny)).astype(dtype) * (rng.random(B) < 0.7)
+        elif kind == 2:  # near the top of the range
+            x[sl] = (rng.standard_normal(B) * float(fi.max) / 4).astype(dtype)
+        elif kind == 3:  # signed zeros
+            x[sl] = np.where(rng.random(B) < 0.5, -0.0, 0.0).astype(dtype)
+        else:            # exponent boundary of the plain range
+            e = -95 if dtype == np.float32 else -959
+            x[sl] = (rng.standard_normal(B) * 2.0 ** e).astype(dtype)
+    return x
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_special_values(cuda, dtype):
+    x = special_values(dtype, 64 * 512 + 13, 5)
+    widths = (4, 8, 9, 16, 21, 24, 31, 32) if dtype == np.float32 else (8, 9, 16, 21, 32, 33, 47, 63, 64)
+    for bits in widths:
+        for E in (8, 32, 64):
+            check(x, bits, E)
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_nan_inf(cuda, dtype):
+    """NaN is skipped by the block max (std::max); +-Inf blocks follow the
+    oracle's definition of the reference's out-of-range shifts."""
+    rng = np.random.default_rng(9)
+    n = 4096 * 3 + 5
+    x = workloads.normal_np(n, dtype, 3)
+    x[rng.choice(n, 40, replace=False)] = np.nan
+    x[rng.choice(n, 10, replace=False)] = np.inf
+    x[rng.choice(n, 10, replace=False)] = -np.inf
+    for bits in ((8, 16, 21, 32) if dtype == np.float32 else (8, 16, 21, 32, 40, 64)):
+        for E in (8, 32):
+            check(x, bits, E)
