@@ -50,12 +50,20 @@ WORKLOADS = {
     "loguniform_f64_2p28_b21_e64": ("loguniform", "float64", 1 << 28, 21, 64),
     "loguniform_f64_2p28_b32_e64": ("loguniform", "float64", 1 << 28, 32, 64),
     "normal_f64_2p20_b32_e32": ("normal", "float64", 1 << 20, 32, 32),
+    # smaller cases (still larger than L2) for ncu captures
+    "loguniform_f64_2p25_b21_e32": ("loguniform", "float64", 1 << 25, 21, 32),
+    "loguniform_f64_2p25_b16_e64": ("loguniform", "float64", 1 << 25, 16, 64),
 }
 DEFAULT_WORKLOAD = "field512_f32_b16_e32"
 
 # DRAM bytes (read + write) per launch from ncu captures, by (workload, kernel);
 # profiles/ holds the captures' summaries and the commands that made them.
-NCU_TRAFFIC = {}
+NCU_TRAFFIC = {
+    ("field512_f32_b16_e32", "compress"): 780_571_136,
+    ("field512_f32_b16_e32", "decompress"): 755_632_128,
+    ("loguniform_f64_2p25_b21_e32", "compress"): 338_155_520,
+    ("loguniform_f64_2p25_b21_e32", "decompress"): 301_903_616,
+}
 
 
 def algorithmic_bytes(dtype: str, n: int, bits: int, E: int) -> int:

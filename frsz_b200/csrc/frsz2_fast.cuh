@@ -30,7 +30,7 @@
 
 namespace frsz2b {
 
-template<class T, int BITS>
+template<class T, int BITS, int NT_ = kNT, int RPW_ = 2>
 struct fast_cfg
 {
   using U = typename fp<T>::U;
@@ -40,12 +40,19 @@ struct fast_cfg
   static constexpr int NW = (L + 31) / 32;       // segment words
   static constexpr bool ALIGNED = (L % 32) == 0; // segments start on word boundaries
   static constexpr int ROW = 32 * P;             // values per warp row
-  static constexpr int RPW = 2;                  // rows per warp per tile
-  static constexpr int WARPS = kNT / 32;
+  static constexpr int NT = NT_;                 // threads per CTA
+  static constexpr int RPW = RPW_;               // rows per warp per tile
+  static constexpr int WARPS = NT / 32;
   static constexpr int ROWS = WARPS * RPW;       // rows per tile
   static constexpr int TE = ROWS * ROW;          // values per tile
   static constexpr int W = BITS <= 8 ? 8 : BITS <= 16 ? 16 : BITS <= 32 ? 32 : 64;
 };
+
+// Values per tile of the fast kernels for a CTA width and rows per warp.
+__host__ __device__ constexpr int fast_tile_values(int dtype_bytes, int nt, int rpw)
+{
+  return (nt / 32) * rpw * 32 * (32 / dtype_bytes);
+}
 
 // ---------------------------------------------------------------- PTX helpers
 
@@ -283,16 +290,17 @@ __device__ __forceinline__ typename fp<T>::U decode_plain(typename fast_cfg<T, B
 
 // ---------------------------------------------------------------- compress
 
-template<class T, int BITS>
-__global__ void __launch_bounds__(kNT) k_compress_fast(Job j)
+// One tile of compress.  s_rmax: 2 * Cfg::ROWS words of shared memory (used
+// only when an exponent block spans several warp rows).
+template<class T, int BITS, int NT, int RPW_>
+__device__ __forceinline__ void fast_compress_tile(const Job& j, std::uint64_t tile, std::uint32_t* s_rmax)
 {
-  using Cfg = fast_cfg<T, BITS>;
+  using Cfg = fast_cfg<T, BITS, NT, RPW_>;
   using U = typename Cfg::U;
   using C = typename Cfg::C;
   using K = key_of<T>;
   constexpr int P = Cfg::P, L = Cfg::L, NW = Cfg::NW, ROW = Cfg::ROW, RPW = Cfg::RPW, TE = Cfg::TE,
                 W = Cfg::W;
-  __shared__ std::uint32_t s_rmax[2][Cfg::ROWS];
 
   const T* __restrict__ x = static_cast<const T*>(j.values_in);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -300,7 +308,7 @@ __global__ void __launch_bounds__(kNT) k_compress_fast(Job j)
   const int G = E / P; // lanes per exponent block
   const int TB = (int)j.tile_blocks;
 
-  for (std::uint64_t tile = blockIdx.x; tile < j.tiles; tile += gridDim.x) {
+  {
     const std::uint64_t e0 = tile * (std::uint64_t)TE;
     const std::uint64_t rem64 = j.n - e0;
     const bool full = rem64 >= (std::uint64_t)TE;
@@ -371,8 +379,8 @@ __global__ void __launch_bounds__(kNT) k_compress_fast(Job j)
         const std::uint32_t a = __reduce_max_sync(0xFFFFFFFFu, km[rr]);
         const std::uint32_t b = __reduce_max_sync(0xFFFFFFFFu, kc[rr]);
         if (lane == 0) {
-          s_rmax[0][rr * Cfg::WARPS + warp] = a;
-          s_rmax[1][rr * Cfg::WARPS + warp] = b;
+          s_rmax[rr * Cfg::WARPS + warp] = a;
+          s_rmax[Cfg::ROWS + rr * Cfg::WARPS + warp] = b;
         }
       }
       __syncthreads();
@@ -382,8 +390,8 @@ __global__ void __launch_bounds__(kNT) k_compress_fast(Job j)
         const int row0 = ((rr * Cfg::WARPS + warp) / rpb) * rpb;
         std::uint32_t a = 0, b = 0;
         for (int q = 0; q < rpb; ++q) {
-          a = max(a, s_rmax[0][row0 + q]);
-          b = max(b, s_rmax[1][row0 + q]);
+          a = max(a, s_rmax[row0 + q]);
+          b = max(b, s_rmax[Cfg::ROWS + row0 + q]);
         }
         km[rr] = a;
         kc[rr] = b;
@@ -464,12 +472,21 @@ __global__ void __launch_bounds__(kNT) k_compress_fast(Job j)
   }
 }
 
+template<class T, int BITS, int NT = kNT, int RPW = 2>
+__global__ void __launch_bounds__(NT) k_compress_fast(Job j)
+{
+  __shared__ std::uint32_t s_rmax[2 * fast_cfg<T, BITS, NT, RPW>::ROWS];
+  for (std::uint64_t tile = blockIdx.x; tile < j.tiles; tile += gridDim.x)
+    fast_compress_tile<T, BITS, NT, RPW>(j, tile, s_rmax);
+}
+
 // ---------------------------------------------------------------- decompress
 
-template<class T, int BITS>
-__global__ void __launch_bounds__(kNT) k_decompress_fast(Job j)
+// One tile of decompress.
+template<class T, int BITS, int NT, int RPW_>
+__device__ __forceinline__ void fast_decompress_tile(const Job& j, std::uint64_t tile)
 {
-  using Cfg = fast_cfg<T, BITS>;
+  using Cfg = fast_cfg<T, BITS, NT, RPW_>;
   using U = typename Cfg::U;
   using C = typename Cfg::C;
   constexpr int P = Cfg::P, L = Cfg::L, NW = Cfg::NW, ROW = Cfg::ROW, RPW = Cfg::RPW, TE = Cfg::TE,
@@ -480,7 +497,7 @@ __global__ void __launch_bounds__(kNT) k_decompress_fast(Job j)
   const int log2E = j.log2E;
   const int TB = (int)j.tile_blocks;
 
-  for (std::uint64_t tile = blockIdx.x; tile < j.tiles; tile += gridDim.x) {
+  {
     const std::uint64_t e0 = tile * (std::uint64_t)TE;
     const std::uint64_t rem64 = j.n - e0;
     const bool full = rem64 >= (std::uint64_t)TE;
@@ -562,6 +579,13 @@ __global__ void __launch_bounds__(kNT) k_decompress_fast(Job j)
       }
     }
   }
+}
+
+template<class T, int BITS, int NT = kNT, int RPW = 2>
+__global__ void __launch_bounds__(NT) k_decompress_fast(Job j)
+{
+  for (std::uint64_t tile = blockIdx.x; tile < j.tiles; tile += gridDim.x)
+    fast_decompress_tile<T, BITS, NT, RPW>(j, tile);
 }
 
 // Requirements of the fast kernels for (dtype, bits, E) and pointers, beyond
