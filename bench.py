@@ -55,6 +55,7 @@ WORKLOADS = {
     "loguniform_f64_2p25_b16_e64": ("loguniform", "float64", 1 << 25, 16, 64),
 }
 DEFAULT_WORKLOAD = "field512_f32_b16_e32"
+BATCH_WORKLOADS = ("batched4096",)
 
 # DRAM bytes (read + write) per launch from ncu captures, by (workload, kernel);
 # profiles/ holds the captures' summaries and the commands that made them.
@@ -416,13 +417,156 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
     print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------------- batched
+
+def batched_specs(count: int = 4096, seed: int = 7):
+    """Config 4: byte sizes log-uniform in [1 KiB, 64 MiB], 50/50 fp32/fp64,
+    bits uniform over {8, 12, 16, 24, 32}, block 32."""
+    rng = np.random.default_rng(seed)
+    specs = []
+    for _ in range(count):
+        nbytes = math.exp(rng.uniform(math.log(1024), math.log(64 << 20)))
+        is64 = rng.random() < 0.5
+        es = 8 if is64 else 4
+        specs.append(("float64" if is64 else "float32", max(1, int(nbytes) // es), int(rng.choice([8, 12, 16, 24, 32])),
+                      32))
+    return specs
+
+
+def run_batched(args, rank: int, world: int, local_rank: int) -> None:
+    """One step = compress all arrays, then decompress all.  value = the
+    batched plan (one graph launch per direction); the same arrays are also
+    timed with one plain frsz2_compress / frsz2_decompress call per array
+    (eager from the host, and recorded into a CUDA graph)."""
+    import torch
+
+    import frsz_b200
+
+    torch.cuda.set_device(local_rank)
+    specs = batched_specs(seed=args.seed + rank)
+    align = 256
+    off_v, off_c, items = 0, 0, []
+    for dt, n, bits, E in specs:
+        es = 4 if dt == "float32" else 8
+        csize = frsz_b200.compressed_size(dt, bits, E, n)
+        items.append((dt, n, bits, E, off_v, off_c, csize))
+        off_v += -(-n * es // align) * align
+        off_c += -(-csize // align) * align
+    pool_in = torch.empty(off_v, dtype=torch.uint8, device="cuda")
+    pool_out = torch.empty(off_v, dtype=torch.uint8, device="cuda")
+    pool_c = torch.zeros(off_c, dtype=torch.uint8, device="cuda")
+    g = torch.Generator(device="cuda").manual_seed(args.seed + rank)
+    arrays = []
+    total_bytes = 0
+    for dt, n, bits, E, ov, oc, csize in items:
+        tdt = torch.float32 if dt == "float32" else torch.float64
+        es = 4 if dt == "float32" else 8
+        x = pool_in[ov:ov + n * es].view(tdt)
+        x.normal_(generator=g)
+        y = pool_out[ov:ov + n * es].view(tdt)
+        c = pool_c[oc:oc + csize]
+        arrays.append(frsz_b200.BatchArray(values=x, compressed=c, bits=bits, block_size=E, decompressed=y))
+        total_bytes += algorithmic_bytes(dt, n, bits, E)
+    torch.cuda.synchronize()
+    stream = torch.cuda.Stream()  # graph capture needs a non-default stream
+    torch.cuda.set_stream(stream)
+    plan = frsz_b200.BatchPlan(arrays)
+    tune_c = plan.autotune(compress=True, stream=stream)
+    tune_d = plan.autotune(compress=False, stream=stream)
+
+    def timed(fn, k):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(k):
+            fn()
+        b.record(stream)
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / k
+
+    K = args.steps
+    ms_c = timed(lambda: plan.compress(stream), K)
+    ms_d = timed(lambda: plan.decompress(stream), K)
+    # plain per-array calls
+    lib = frsz_b200.lib()
+    sp = stream.cuda_stream
+    plain = [(frsz_b200.codec.dtype_code(a.values.dtype), a.bits, a.block_size, a.values.data_ptr(),
+              a.values.numel(), a.compressed.data_ptr(), a.decompressed.data_ptr()) for a in arrays]
+
+    def per_array_c():
+        for code, bits, E, xp, n, cp, _ in plain:
+            lib.frsz2_compress(code, bits, E, xp, n, cp, sp)
+
+    def per_array_d():
+        for code, bits, E, _, n, cp, yp in plain:
+            lib.frsz2_decompress(code, bits, E, cp, n, yp, sp)
+
+    K2 = max(1, min(K, 5))
+    ms_pc = timed(per_array_c, K2)
+    ms_pd = timed(per_array_d, K2)
+    graphs = []
+    for fn in (per_array_c, per_array_d):
+        gr = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(gr, stream=stream):
+            fn()
+        graphs.append(gr)
+    ms_gc = timed(graphs[0].replay, K2)
+    ms_gd = timed(graphs[1].replay, K2)
+    del graphs
+    # parity spot check of a few arrays against the oracle
+    import oracle
+    rng = np.random.default_rng(1)
+    for i in rng.choice(len(arrays), 6, replace=False):
+        a = arrays[int(i)]
+        if a.values.numel() > (1 << 22):
+            continue
+        xh = a.values.cpu().numpy()
+        ref = oracle.compress(xh, a.bits, a.block_size, canary=0)
+        got = a.compressed.cpu().numpy()
+        w = frsz_b200.word_bits(a.bits) // 8
+        nb = -(-xh.size // a.block_size)
+        assert np.array_equal(got[:nb * w], ref[:nb * w]), "batched exponents differ from the oracle"
+        eb = frsz_b200.exponent_size(xh.dtype, a.bits, a.block_size, xh.size)
+        assert np.array_equal(got[eb:], ref[eb:]), "batched words differ from the oracle"
+    info = plan.info()
+    if rank != 0:
+        return
+    step_ms = ms_c + ms_d
+    value = world * 2 * total_bytes / (step_ms / 1e3) / 1e9
+    per_ms = ms_pc + ms_pd
+    gper_ms = ms_gc + ms_gd
+    peaks = load_peaks()
+    line = {
+        "metric": METRIC, "value": round(value, 3), "unit": "GB/s", "n_gpus": world, "steps": K,
+        "warmup": args.warmup, "ms_per_step": round(step_ms, 4), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u32/u64", "data": "synthetic",
+        "config": {"workload": "batched4096", "arrays": len(arrays), "bytes_per_step": 2 * total_bytes,
+                   "sizes": "log-uniform 1 KiB-64 MiB", "dtypes": "50/50 fp32/fp64 N(0,1)",
+                   "bits": [8, 12, 16, 24, 32], "block_size": 32, "l2": "inputs larger than L2, no flush"},
+        "batched": {"compress_gbs": round(total_bytes / ms_c / 1e6, 1),
+                    "decompress_gbs": round(total_bytes / ms_d / 1e6, 1),
+                    "hbm_frac": round(2 * total_bytes / step_ms / 1e6 / peaks["hbm_gbs"], 4),
+                    "autotune_ms": {"compress": round(tune_c, 4), "decompress": round(tune_d, 4)},
+                    "plan": info},
+        "per_array_plain": {"gbs": round(2 * total_bytes / per_ms / 1e6, 1), "ms_per_step": round(per_ms, 3),
+                            "launches_per_step": 2 * len(arrays), "host_loop": "python ctypes"},
+        "per_array_graph": {"gbs": round(2 * total_bytes / gper_ms / 1e6, 1), "ms_per_step": round(gper_ms, 3)},
+        "speedup_vs_per_array_plain": round(per_ms / step_ms, 2),
+        "speedup_vs_per_array_graph": round(gper_ms / step_ms, 2),
+        "gpu_launches": 2 * info["classes"] * K,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS), default=DEFAULT_WORKLOAD)
+    ap.add_argument("--workload", choices=sorted(WORKLOADS) + list(BATCH_WORKLOADS), default=DEFAULT_WORKLOAD)
     ap.add_argument("--seed", type=int, default=42)
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--cpu-seconds", type=float, default=3.0)
@@ -433,7 +577,9 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
-    if args.impl == "reference":
+    if args.workload in BATCH_WORKLOADS:
+        run_batched(args, rank, world, local_rank)
+    elif args.impl == "reference":
         run_reference_arm(args, rank, world)
     else:
         run_ours(args, rank, world, local_rank)

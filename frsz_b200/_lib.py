@@ -22,6 +22,22 @@ _u64 = ctypes.c_uint64
 _vp = ctypes.c_void_p
 _int = ctypes.c_int
 
+class BatchItemC(ctypes.Structure):
+    """frsz2_batch_item (include/frsz2_b200.h)."""
+    _fields_ = [("dtype", ctypes.c_int), ("bits", ctypes.c_int), ("block_size", ctypes.c_int),
+                ("n", ctypes.c_uint64), ("values", ctypes.c_void_p), ("decompressed", ctypes.c_void_p),
+                ("compressed", ctypes.c_void_p)]
+
+
+class BatchStatsC(ctypes.Structure):
+    """frsz2_batch_stats (include/frsz2_b200.h)."""
+    _fields_ = [("arrays", ctypes.c_uint64), ("persistent_arrays", ctypes.c_uint64),
+                ("separate_launches", ctypes.c_uint64), ("classes", ctypes.c_uint64),
+                ("tiles", ctypes.c_uint64 * 2), ("threads_per_cta", ctypes.c_int * 2),
+                ("rows_per_warp", ctypes.c_int * 2), ("ctas_per_sm", ctypes.c_int * 2),
+                ("side_by_side", ctypes.c_int * 2), ("tuned", ctypes.c_int * 2)]
+
+
 # name -> (restype, argtypes); kept in step with include/frsz2_b200.h
 SIGNATURES = {
     "register_frsz": (None, []),
@@ -34,6 +50,12 @@ SIGNATURES = {
     "frsz2_compress_host": (_int, [_int, _int, _int, _vp, _u64, _vp, _vp]),
     "frsz2_decompress_host": (_int, [_int, _int, _int, _vp, _u64, _vp, _vp]),
     "frsz2_decompress_elements": (_int, [_int, _int, _int, _vp, _u64, _vp, _u64, _vp, _vp]),
+    "frsz2_batch_create": (_int, [ctypes.POINTER(BatchItemC), _u64, ctypes.POINTER(_vp)]),
+    "frsz2_batch_compress": (_int, [_vp, _vp]),
+    "frsz2_batch_decompress": (_int, [_vp, _vp]),
+    "frsz2_batch_autotune": (_int, [_vp, _int, _vp, ctypes.POINTER(ctypes.c_float)]),
+    "frsz2_batch_info": (_int, [_vp, ctypes.POINTER(BatchStatsC)]),
+    "frsz2_batch_destroy": (None, [_vp]),
 }
 
 

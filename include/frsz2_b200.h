@@ -93,6 +93,54 @@ int frsz2_decompress_host(int dtype, int bits, int block_size, const void* h_com
 int frsz2_decompress_elements(int dtype, int bits, int block_size, const void* d_compressed, uint64_t n,
                               const uint64_t* d_idx, uint64_t count, void* d_out, void* stream);
 
+/* ---------------------------------------------------------------------------
+ * Batched path: no counterpart in the reference (which compresses one array
+ * per call).  Many arrays of mixed float types, widths, block sizes and sizes
+ * run as one CUDA graph launch: a persistent kernel per (float type, width)
+ * class present, side by side, each walking its class's work list in device
+ * memory.  The launch shape (threads per CTA, rows per warp, resident CTAs
+ * per SM, classes side by side or one after another) comes from an autotuner
+ * that times the candidates on the plan's own arrays.  Arrays the persistent
+ * kernels cannot take (block sizes that are not powers of two, block padding,
+ * misaligned pointers) get their own launch inside the same graph.  All
+ * pointers are device pointers; a plan keeps its descriptors in device memory
+ * until destroyed.
+ */
+typedef struct frsz2_batch_item {
+  int dtype;              /* FRSZ2_FLOAT / FRSZ2_DOUBLE */
+  int bits;
+  int block_size;
+  uint64_t n;
+  const void* values;     /* compress input (may be NULL for a decompress-only plan) */
+  void* decompressed;     /* decompress output (may be NULL for a compress-only plan; may equal values) */
+  void* compressed;       /* frsz2_compressed_size() bytes */
+} frsz2_batch_item;
+
+typedef struct frsz2_batch frsz2_batch;
+
+typedef struct frsz2_batch_stats {
+  uint64_t arrays;            /* items in the plan */
+  uint64_t persistent_arrays; /* items served by the persistent kernels */
+  uint64_t separate_launches; /* items with their own launch in the graph */
+  uint64_t classes;           /* (float type, width) classes = persistent kernels */
+  uint64_t tiles[2];          /* persistent-kernel tiles [decompress, compress] */
+  int threads_per_cta[2];
+  int rows_per_warp[2];
+  int ctas_per_sm[2];
+  int side_by_side[2];        /* 1: classes run concurrently, 0: one after another */
+  int tuned[2];
+} frsz2_batch_stats;
+
+int frsz2_batch_create(const frsz2_batch_item* items, uint64_t count, frsz2_batch** plan);
+int frsz2_batch_compress(frsz2_batch* plan, void* stream);
+int frsz2_batch_decompress(frsz2_batch* plan, void* stream);
+/* Times every launch shape on the plan's arrays for one direction (compress != 0
+ * or decompress), keeps the fastest and rebuilds that direction's graph.  The
+ * run writes the plan's outputs like a normal call.  *best_ms may be NULL. */
+int frsz2_batch_autotune(frsz2_batch* plan, int compress, void* stream, float* best_ms);
+int frsz2_batch_info(const frsz2_batch* plan, frsz2_batch_stats* stats);
+void frsz2_batch_destroy(frsz2_batch* plan);
+
 #ifdef __cplusplus
 }
 #endif
