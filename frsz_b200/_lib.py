@@ -56,6 +56,7 @@ SIGNATURES = {
     "frsz2_batch_autotune": (_int, [_vp, _int, _vp, ctypes.POINTER(ctypes.c_float)]),
     "frsz2_batch_info": (_int, [_vp, ctypes.POINTER(BatchStatsC)]),
     "frsz2_batch_destroy": (None, [_vp]),
+    "frsz2_batch_compress_static": (_int, [ctypes.POINTER(BatchItemC), _u64, _vp]),
 }
 
 

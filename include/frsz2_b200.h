@@ -141,6 +141,19 @@ int frsz2_batch_autotune(frsz2_batch* plan, int compress, void* stream, float* b
 int frsz2_batch_info(const frsz2_batch* plan, frsz2_batch_stats* stats);
 void frsz2_batch_destroy(frsz2_batch* plan);
 
+/* Batched compress that allocates nothing (no counterpart in the reference).
+ * For callers that may not allocate device memory at call time -- an
+ * application whose allocator already owns the GPU's memory, or a request path
+ * where a cudaMalloc is not allowed.  Same output as a plan built from the same
+ * items and run with frsz2_batch_compress; `items` is host memory and the
+ * `decompressed` fields are ignored.  The descriptor work list lives in a fixed
+ * device array of the library (4096 arrays at most per call; larger calls
+ * return 2), held by every GPU that loads the library until exit, shared by
+ * all calls: calls whose work overlaps on the GPU (other streams or threads)
+ * race.  The first call on each device sets the array up; make it before any
+ * stream capture. */
+int frsz2_batch_compress_static(const frsz2_batch_item* items, uint64_t count, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
