@@ -246,6 +246,13 @@ int frsz2_batch_create(const frsz2_batch_item* items, uint64_t count, frsz2_batc
     int rc = check_args(it.dtype, it.bits, it.block_size);
     if (!rc && it.n > 0 && (!it.compressed || (!it.values && !it.decompressed)))
       rc = set_error(FRSZ2_EFAIL, "null pointer in batch item " + std::to_string(i));
+    const std::uintptr_t es = it.dtype == FRSZ2_DOUBLE ? 8 : 4;
+    const std::uintptr_t ws = (std::uintptr_t)word_bits(it.bits) / 8;
+    if (!rc && it.n > 0 &&
+        (reinterpret_cast<std::uintptr_t>(it.values) % es != 0 ||
+         reinterpret_cast<std::uintptr_t>(it.decompressed) % es != 0 ||
+         reinterpret_cast<std::uintptr_t>(it.compressed) % ws != 0))
+      rc = set_error(FRSZ2_EFAIL, "misaligned pointer in batch item " + std::to_string(i));
     if (rc) {
       delete p;
       return rc;

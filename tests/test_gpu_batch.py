@@ -97,3 +97,10 @@ def test_batch_direction_checks(cuda):
     plan2 = BatchPlan([BatchArray(values=None, compressed=buf, bits=16, block_size=32, decompressed=x)])
     with pytest.raises(frsz_b200.Frsz2Error, match="compress-only|decompress-only"):
         plan2.compress()
+
+
+def test_batch_rejects_misaligned_pointers(cuda):
+    x = torch.zeros(101, dtype=torch.float64, device="cuda")
+    buf = torch.zeros(frsz_b200.compressed_size(np.float64, 32, 32, 100) + 8, dtype=torch.uint8, device="cuda")
+    with pytest.raises(frsz_b200.Frsz2Error, match="misaligned"):
+        BatchPlan([BatchArray(values=x[1:], compressed=buf[2:], bits=32, block_size=32)])
