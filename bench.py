@@ -55,7 +55,7 @@ WORKLOADS = {
     "loguniform_f64_2p25_b16_e64": ("loguniform", "float64", 1 << 25, 16, 64),
 }
 DEFAULT_WORKLOAD = "field512_f32_b16_e32"
-BATCH_WORKLOADS = ("batched4096",)
+BATCH_WORKLOADS = ("batched4096", "krylov100")
 
 # DRAM bytes (read + write) per launch from ncu captures, by (workload, kernel);
 # profiles/ holds the captures' summaries and the commands that made them.
@@ -560,6 +560,88 @@ def run_batched(args, rank: int, world: int, local_rank: int) -> None:
     print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------------- fused basis
+
+def run_krylov(args, rank: int, world: int, local_rank: int) -> None:
+    """Config 3b: 100 fp64 vectors of 2^22 values, 32 bits, block 32.  Times
+    the fused h = V^T w and y += V c over the compressed basis, against
+    decompress-then-torch and against torch on the uncompressed basis."""
+    import torch
+
+    import frsz_b200
+
+    torch.cuda.set_device(local_rank)
+    m, n, bits, E = 100, 1 << 22, 32, 32
+    g = torch.Generator(device="cuda").manual_seed(args.seed + rank)
+    V = torch.randn(m, n, generator=g, device="cuda", dtype=torch.float64)
+    basis = frsz_b200.CompressedBasis(m, n, bits=bits, block_size=E)
+    for j in range(m):
+        basis.append(V[j])
+    Vd = torch.stack([basis.get(j) for j in range(m)])  # decompressed basis, for the checks and baselines
+    w = torch.randn(n, generator=g, device="cuda", dtype=torch.float64)
+    c = torch.randn(m, generator=g, device="cuda", dtype=torch.float64)
+    y = torch.randn(n, generator=g, device="cuda", dtype=torch.float64)
+    stream = torch.cuda.current_stream()
+    tmp = torch.empty(n, dtype=torch.float64, device="cuda")
+    h = torch.empty(m, dtype=torch.float64, device="cuda")
+
+    def timed(fn, k):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(k):
+            fn()
+        b.record(stream)
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / k
+
+    def unfused_dot():
+        for j in range(m):
+            frsz_b200.decompress(basis.buffers[j], n, torch.float64, bits, E, out=tmp)
+            h[j] = torch.dot(tmp, w)
+
+    K = args.steps
+    ms_dot = timed(lambda: basis.dot(w, out=h), K)
+    ms_axpy = timed(lambda: basis.axpy(c, y), K)
+    ms_unfused = timed(unfused_dot, max(1, K // 10))
+    ms_dense_dot = timed(lambda: torch.mv(V, w, out=h), K)
+    ms_dense_axpy = timed(lambda: y.addmv_(V.t(), c), K)
+    # accuracy of the fused results against torch on the decompressed basis
+    hd = basis.dot(w)
+    dot_err = float(((hd - Vd @ w).abs() / (Vd.abs() @ w.abs())).max())
+    y0 = torch.randn(n, generator=g, device="cuda", dtype=torch.float64)
+    y1 = y0.clone()
+    basis.axpy(c, y1)
+    axpy_err = float(((y1 - (y0 + c @ Vd)).abs() / (y0.abs() + c.abs() @ Vd.abs())).max())
+    comp_bytes = m * frsz_b200.compressed_size(np.float64, bits, E, n)
+    dot_bytes = m * algorithmic_bytes("float64", n, bits, E) - m * n * 8 + n * 8
+    axpy_bytes = dot_bytes + n * 8
+    peaks = load_peaks()
+    if rank != 0:
+        return
+    value = world * (dot_bytes + axpy_bytes) / ((ms_dot + ms_axpy) / 1e3) / 1e9
+    line = {
+        "metric": METRIC, "value": round(value, 3), "unit": "GB/s", "n_gpus": world, "steps": K,
+        "warmup": args.warmup, "ms_per_step": round(ms_dot + ms_axpy, 4), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "krylov100", "vectors": m, "n": n, "bits": bits, "block_size": E,
+                   "compressed_basis_bytes": comp_bytes, "step": "fused dot h=V^T w, then fused axpy y+=V c"},
+        "fused_dot": {"ms": round(ms_dot, 4), "gbs": round(dot_bytes / ms_dot / 1e6, 1),
+                      "hbm_frac": round(dot_bytes / ms_dot / 1e6 / peaks["hbm_gbs"], 4), "max_rel_err": dot_err},
+        "fused_axpy": {"ms": round(ms_axpy, 4), "gbs": round(axpy_bytes / ms_axpy / 1e6, 1),
+                       "hbm_frac": round(axpy_bytes / ms_axpy / 1e6 / peaks["hbm_gbs"], 4),
+                       "max_rel_err": axpy_err},
+        "decompress_then_dot_ms": round(ms_unfused, 4),
+        "uncompressed_torch": {"dot_ms": round(ms_dense_dot, 4), "axpy_ms": round(ms_dense_axpy, 4)},
+        "speedup_fused_dot_vs_uncompressed": round(ms_dense_dot / ms_dot, 2),
+        "speedup_fused_axpy_vs_uncompressed": round(ms_dense_axpy / ms_axpy, 2),
+        "gpu_launches": 2 * K,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
     ap.add_argument("--gpus", type=int, default=1)
@@ -577,8 +659,10 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
-    if args.workload in BATCH_WORKLOADS:
+    if args.workload == "batched4096":
         run_batched(args, rank, world, local_rank)
+    elif args.workload == "krylov100":
+        run_krylov(args, rank, world, local_rank)
     elif args.impl == "reference":
         run_reference_arm(args, rank, world)
     else:

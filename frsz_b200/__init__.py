@@ -22,10 +22,11 @@ from .codec import (
 )
 from .plugin import Frsz2Plugin
 from .batch import BatchArray, BatchPlan
+from .krylov import CompressedBasis
 
 __all__ = [
     "FRSZ2_DOUBLE", "FRSZ2_EDTYPE", "FRSZ2_EFAIL", "FRSZ2_FLOAT", "FRSZ2_OK", "Frsz2Error", "lib",
     "Frsz2Compressor", "compress", "compress_host", "compressed_size", "decompress", "decompress_elements",
     "decompress_host", "dispatch_frsz2_compression", "dispatch_frsz2_decompression", "exponent_size", "word_bits",
-    "Frsz2Plugin", "BatchArray", "BatchPlan",
+    "Frsz2Plugin", "BatchArray", "BatchPlan", "CompressedBasis",
 ]

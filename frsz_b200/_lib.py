@@ -57,6 +57,9 @@ SIGNATURES = {
     "frsz2_batch_info": (_int, [_vp, ctypes.POINTER(BatchStatsC)]),
     "frsz2_batch_destroy": (None, [_vp]),
     "frsz2_batch_compress_static": (_int, [ctypes.POINTER(BatchItemC), _u64, _vp]),
+    "frsz2_basis_workspace_size": (_u64, [_int, _u64]),
+    "frsz2_basis_dot": (_int, [_int, _int, _int, ctypes.POINTER(_vp), _int, _u64, _vp, _vp, _vp, _u64, _vp]),
+    "frsz2_basis_axpy": (_int, [_int, _int, _int, ctypes.POINTER(_vp), _int, _u64, _vp, _vp, _vp]),
 }
 
 

@@ -604,3 +604,120 @@ __host__ inline bool fast_eligible(const Job& j, int dtype_is_f64, const void* v
 }
 
 } // namespace frsz2b
+
+namespace frsz2b {
+
+// Raw words and block exponent of one lane's P values, loaded ahead of the
+// decode so a consumer can keep several lanes' loads in flight.
+template<class T, int BITS>
+struct lane_words
+{
+  std::uint32_t w[fast_cfg<T, BITS>::NW + 1];
+  std::int64_t be;
+  int o; // bit offset of the segment in w[0]
+};
+
+template<class T, int BITS>
+__device__ __forceinline__ void fast_load_lane(const std::uint8_t* __restrict__ exps,
+                                               const std::uint8_t* __restrict__ words, int log2E, std::uint64_t idx,
+                                               lane_words<T, BITS>& lw)
+{
+  using Cfg = fast_cfg<T, BITS>;
+  constexpr int L = Cfg::L, NW = Cfg::NW, W = Cfg::W;
+  lw.be = load_exp(exps + (idx >> log2E) * (std::uint64_t)(W / 8), W);
+  const std::uint64_t S = idx * (std::uint64_t)BITS;
+  const std::uint32_t* src = reinterpret_cast<const std::uint32_t*>(words) + (S >> 5);
+  lw.o = (int)(S & 31u);
+  if constexpr (Cfg::ALIGNED) {
+    std::uint32_t t[NW];
+    load_words<NW>(src, t);
+#pragma unroll
+    for (int i = 0; i < NW; ++i) lw.w[i] = t[i];
+    lw.w[NW] = 0;
+  } else {
+#pragma unroll
+    for (int i = 0; i < NW; ++i) lw.w[i] = __ldg(src + i);
+    lw.w[NW] = (lw.o + L > 32 * NW) ? __ldg(src + NW) : 0u;
+  }
+}
+
+template<class T, int BITS>
+__device__ __forceinline__ void fast_decode_loaded(const lane_words<T, BITS>& lw, T (&out)[fast_cfg<T, BITS>::P])
+{
+  using Cfg = fast_cfg<T, BITS>;
+  using U = typename Cfg::U;
+  using C = typename Cfg::C;
+  constexpr int P = Cfg::P, NW = Cfg::NW;
+  std::uint32_t seg[NW + 1];
+  if constexpr (Cfg::ALIGNED) {
+#pragma unroll
+    for (int i = 0; i <= NW; ++i) seg[i] = lw.w[i];
+  } else {
+#pragma unroll
+    for (int i = 0; i < NW; ++i) seg[i] = __funnelshift_r(lw.w[i], lw.w[i + 1], lw.o);
+    seg[NW] = 0;
+  }
+  C c[P];
+  unpack_all<0, BITS>(seg, c);
+  const std::int64_t be = lw.be;
+  if (plain_exponent<T>(be)) {
+    const T inv = pow2<T>((int)be - BITS + 2);
+    const U zero_bits =
+      sizeof(T) == 4 ? (U)((std::uint32_t)(be + 96) << 23) : (U)((std::uint64_t)(be + 992) << 52);
+#pragma unroll
+    for (int i = 0; i < P; ++i) out[i] = from_bits<T>(decode_plain<T, BITS>(c[i], inv, zero_bits));
+  } else {
+#pragma unroll
+    for (int i = 0; i < P; ++i) out[i] = from_code<T>((U)c[i], be, BITS);
+  }
+}
+
+// Decode the P values of one array that start at element idx (a multiple of
+// P), for consumers that use the values in registers (fused kernels).  The
+// array's stream must be contiguous (E * bits a multiple of W, E a power of
+// two >= P); values at or beyond the array's end come out as garbage and must
+// be ignored by the caller.
+template<class T, int BITS>
+__device__ __forceinline__ void fast_decode_lane(const std::uint8_t* __restrict__ exps,
+                                                 const std::uint8_t* __restrict__ words, int log2E,
+                                                 std::uint64_t idx, T (&out)[fast_cfg<T, BITS>::P])
+{
+  using Cfg = fast_cfg<T, BITS>;
+  using U = typename Cfg::U;
+  using C = typename Cfg::C;
+  constexpr int P = Cfg::P, L = Cfg::L, NW = Cfg::NW, W = Cfg::W;
+  const std::int64_t be = load_exp(exps + (idx >> log2E) * (std::uint64_t)(W / 8), W);
+  const std::uint64_t S = idx * (std::uint64_t)BITS;
+  const std::uint32_t* src = reinterpret_cast<const std::uint32_t*>(words) + (S >> 5);
+  std::uint32_t seg[NW + 1];
+  if constexpr (Cfg::ALIGNED) {
+    std::uint32_t t[NW];
+    load_words<NW>(src, t);
+#pragma unroll
+    for (int i = 0; i < NW; ++i) seg[i] = t[i];
+    seg[NW] = 0;
+  } else {
+    const int o = (int)(S & 31u);
+    std::uint32_t wv[NW + 1];
+#pragma unroll
+    for (int i = 0; i < NW; ++i) wv[i] = __ldg(src + i);
+    wv[NW] = (o + L > 32 * NW) ? __ldg(src + NW) : 0u;
+#pragma unroll
+    for (int i = 0; i < NW; ++i) seg[i] = __funnelshift_r(wv[i], wv[i + 1], o);
+    seg[NW] = 0;
+  }
+  C c[P];
+  unpack_all<0, BITS>(seg, c);
+  if (plain_exponent<T>(be)) {
+    const T inv = pow2<T>((int)be - BITS + 2);
+    const U zero_bits =
+      sizeof(T) == 4 ? (U)((std::uint32_t)(be + 96) << 23) : (U)((std::uint64_t)(be + 992) << 52);
+#pragma unroll
+    for (int i = 0; i < P; ++i) out[i] = from_bits<T>(decode_plain<T, BITS>(c[i], inv, zero_bits));
+  } else {
+#pragma unroll
+    for (int i = 0; i < P; ++i) out[i] = from_code<T>((U)c[i], be, BITS);
+  }
+}
+
+} // namespace frsz2b

@@ -1,0 +1,303 @@
+// frsz2_krylov.cu -- decompress fused into its consumer: dot products and
+// axpy over a basis of FRSZ2-compressed fp64 vectors (the compressed Krylov
+// basis use of the reference's random-access decode,
+// include/frsz2.hpp:1096-1104).  Values are decoded in registers straight into
+// the FMAs and never written back.
+//
+//   frsz2_basis_dot:  h[j] = sum_i V_j[i] * w[i]           j < m
+//   frsz2_basis_axpy: y[i] = y[i] + sum_j c[j] * V_j[i]     (j in order 0..m-1)
+//
+// dot: CTA b owns a contiguous element range; it stages its slice of w in
+// shared memory once and streams every basis vector's slice through it (the
+// basis and w are each read once).  Per-warp partial sums per vector go to
+// shared memory; each CTA writes its m partials to the caller's workspace and
+// the last CTA to finish (a ticket counter in the workspace) adds them in CTA
+// order, so the result does not depend on scheduling.
+#include "frsz2_fast.cuh"
+#include "frsz2_launch.hpp"
+
+#include "../../include/frsz2_b200.h"
+
+#include <algorithm>
+#include <string>
+
+namespace frsz2b {
+namespace {
+
+constexpr int kMaxBasis = FRSZ2_MAX_BASIS;
+constexpr int kKT = 256;            // threads per CTA
+constexpr int kSub = 3072;          // w values staged per step (24 KiB)
+constexpr int kJB = 8;              // basis vectors whose loads are in flight together
+
+struct BasisParams
+{
+  const std::uint8_t* buf[kMaxBasis]; // compressed vectors
+};
+
+struct BasisGeo
+{
+  std::uint64_t n;
+  std::uint64_t exp_bytes;
+  int log2E;
+};
+
+template<int BITS>
+__global__ void __launch_bounds__(kKT)
+  k_basis_dot(const __grid_constant__ BasisParams bp, int m, BasisGeo g, const double* __restrict__ w,
+              std::uint64_t chunk, double* __restrict__ partials, unsigned int* __restrict__ ticket,
+              double* __restrict__ h)
+{
+  constexpr int P = fast_cfg<double, BITS>::P;
+  __shared__ double s_w[kSub];
+  __shared__ double s_acc[kKT / 32][kMaxBasis];
+  __shared__ bool s_last;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  for (int j = lane; j < m; j += 32) s_acc[warp][j] = 0.0;
+
+  const std::uint64_t c0 = (std::uint64_t)blockIdx.x * chunk;
+  const std::uint64_t c1 = c0 + chunk < g.n ? c0 + chunk : g.n;
+  for (std::uint64_t s0 = c0; s0 < c1; s0 += kSub) {
+    const int len = (int)((c1 - s0) < (std::uint64_t)kSub ? (c1 - s0) : (std::uint64_t)kSub);
+    __syncthreads(); // previous slice fully consumed
+    for (int i = tid; i < len; i += kKT) s_w[i] = __ldg(w + s0 + i);
+    __syncthreads();
+    // kJB vectors at a time: all their loads are issued before any decode
+    for (int j0 = 0; j0 < m; j0 += kJB) {
+      double acc[kJB];
+#pragma unroll
+      for (int jj = 0; jj < kJB; ++jj) acc[jj] = 0.0;
+      for (int i = tid * P; i < len; i += kKT * P) {
+        lane_words<double, BITS> lw[kJB];
+#pragma unroll
+        for (int jj = 0; jj < kJB; ++jj)
+          if (j0 + jj < m) {
+            const std::uint8_t* buf = bp.buf[j0 + jj];
+            fast_load_lane<double, BITS>(buf, buf + g.exp_bytes, g.log2E, s0 + (std::uint64_t)i, lw[jj]);
+          }
+        double wv[P];
+#pragma unroll
+        for (int k = 0; k < P; ++k) wv[k] = i + k < len ? s_w[i + k] : 0.0;
+#pragma unroll
+        for (int jj = 0; jj < kJB; ++jj)
+          if (j0 + jj < m) {
+            double v[P];
+            fast_decode_loaded<double, BITS>(lw[jj], v);
+#pragma unroll
+            for (int k = 0; k < P; ++k) acc[jj] = fma(v[k], wv[k], acc[jj]);
+          }
+      }
+#pragma unroll
+      for (int jj = 0; jj < kJB; ++jj) {
+        double a = acc[jj];
+#pragma unroll
+        for (int s = 16; s > 0; s >>= 1) a += __shfl_down_sync(0xFFFFFFFFu, a, s);
+        if (lane == 0 && j0 + jj < m) s_acc[warp][j0 + jj] += a;
+      }
+    }
+  }
+  __syncthreads();
+  for (int j = tid; j < m; j += kKT) {
+    double p = 0.0;
+#pragma unroll
+    for (int q = 0; q < kKT / 32; ++q) p += s_acc[q][j];
+    partials[(std::uint64_t)blockIdx.x * m + j] = p;
+  }
+  __threadfence();
+  __syncthreads();
+  if (tid == 0) s_last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (s_last) {
+    __threadfence();
+    for (int j = tid; j < m; j += kKT) {
+      double sum = 0.0;
+      for (unsigned b = 0; b < gridDim.x; ++b) sum += __ldcg(partials + (std::uint64_t)b * m + j);
+      h[j] = sum;
+    }
+    if (tid == 0) *ticket = 0u; // ready for the next call
+  }
+}
+
+template<int BITS>
+__global__ void __launch_bounds__(kKT)
+  k_basis_axpy(const __grid_constant__ BasisParams bp, int m, BasisGeo g, const double* __restrict__ coef,
+               double* __restrict__ y)
+{
+  constexpr int P = fast_cfg<double, BITS>::P;
+  __shared__ double s_c[kMaxBasis];
+  for (int j = threadIdx.x; j < m; j += kKT) s_c[j] = __ldg(coef + j);
+  __syncthreads();
+  const std::uint64_t stride = (std::uint64_t)gridDim.x * kKT * P;
+  for (std::uint64_t idx = ((std::uint64_t)blockIdx.x * kKT + threadIdx.x) * P; idx < g.n; idx += stride) {
+    const bool whole = idx + P <= g.n;
+    double acc[P];
+    if (whole) {
+      std::uint32_t v[8];
+      ld256_stream(y + idx, v);
+#pragma unroll
+      for (int k = 0; k < P; ++k) acc[k] = __longlong_as_double(((long long)v[2 * k + 1] << 32) | v[2 * k]);
+    } else {
+#pragma unroll
+      for (int k = 0; k < P; ++k) acc[k] = idx + k < g.n ? y[idx + k] : 0.0;
+    }
+    for (int j0 = 0; j0 < m; j0 += kJB) {
+      lane_words<double, BITS> lw[kJB];
+#pragma unroll
+      for (int jj = 0; jj < kJB; ++jj)
+        if (j0 + jj < m) {
+          const std::uint8_t* buf = bp.buf[j0 + jj];
+          fast_load_lane<double, BITS>(buf, buf + g.exp_bytes, g.log2E, idx, lw[jj]);
+        }
+#pragma unroll
+      for (int jj = 0; jj < kJB; ++jj)
+        if (j0 + jj < m) {
+          double v[P];
+          fast_decode_loaded<double, BITS>(lw[jj], v);
+          const double cj = s_c[j0 + jj];
+#pragma unroll
+          for (int k = 0; k < P; ++k) acc[k] = fma(cj, v[k], acc[k]);
+        }
+    }
+    if (whole) {
+      std::uint32_t v[8];
+#pragma unroll
+      for (int k = 0; k < P; ++k) {
+        const unsigned long long b = (unsigned long long)__double_as_longlong(acc[k]);
+        v[2 * k] = (std::uint32_t)b;
+        v[2 * k + 1] = (std::uint32_t)(b >> 32);
+      }
+      st256_stream(y + idx, v);
+    } else {
+      for (int k = 0; k < P && idx + k < g.n; ++k) y[idx + k] = acc[k];
+    }
+  }
+}
+
+// widths with fused kernels (fp64 bases)
+#define FRSZ2_KRYLOV_WIDTHS(X) X(16) X(21) X(24) X(32) X(48) X(64)
+
+int basis_args(int dtype, int bits, int E, const void* const* basis, int m, std::uint64_t n, BasisParams* bp,
+               BasisGeo* g)
+{
+  if (int rc = check_args(dtype, bits, E)) return rc;
+  if (dtype != FRSZ2_DOUBLE) return set_error(FRSZ2_EFAIL, "fused basis kernels take fp64 bases");
+  switch (bits) {
+#define CASE(B) case B:
+    FRSZ2_KRYLOV_WIDTHS(CASE)
+#undef CASE
+    break;
+    default: return set_error(FRSZ2_EFAIL, "fused basis kernels have no instance for " + std::to_string(bits) + " bits");
+  }
+  if (E < 4 || E > 65536 || (E & (E - 1)) != 0 || ((std::uint64_t)E * bits) % word_bits(bits) != 0)
+    return set_error(FRSZ2_EFAIL, "fused basis kernels need a power-of-two block size without block padding");
+  if (m < 0 || m > kMaxBasis)
+    return set_error(FRSZ2_EFAIL, "basis size must be in [0, " + std::to_string(kMaxBasis) + "]");
+  if (m > 0 && !basis) return set_error(FRSZ2_EFAIL, "null basis");
+  const Layout L = make_layout(n, bits, E);
+  for (int j = 0; j < m; ++j) {
+    if (!basis[j] || reinterpret_cast<std::uintptr_t>(basis[j]) % 32 != 0)
+      return set_error(FRSZ2_EFAIL, "basis vector " + std::to_string(j) + " is null or not 32-byte aligned");
+    bp->buf[j] = static_cast<const std::uint8_t*>(basis[j]);
+  }
+  g->n = n;
+  g->exp_bytes = L.exp_bytes;
+  int l = 0;
+  while ((1 << l) < E) ++l;
+  g->log2E = l;
+  return FRSZ2_OK;
+}
+
+constexpr int kMaxCtasPerSm = 8; // bound used to size the workspace
+
+// Values per CTA for `ctas` resident CTAs: a multiple of 256 (whole lanes).
+std::uint64_t dot_chunk(std::uint64_t n, std::uint64_t ctas)
+{
+  std::uint64_t chunk = (n + ctas - 1) / ctas;
+  return std::max<std::uint64_t>(256, ((chunk + 255) / 256) * 256);
+}
+
+template<int BITS>
+int dot_ctas_per_sm()
+{
+  int blocks = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k_basis_dot<BITS>, kKT, 0) != cudaSuccess || blocks < 1)
+    blocks = 1;
+  return std::min(blocks, kMaxCtasPerSm);
+}
+
+} // namespace
+} // namespace frsz2b
+
+using namespace frsz2b;
+
+extern "C" {
+
+uint64_t frsz2_basis_workspace_size(int m, uint64_t n)
+{
+  (void)n;
+  if (m < 0) m = 0;
+  const std::uint64_t grid = (std::uint64_t)sm_count() * kMaxCtasPerSm;
+  return 256 + grid * (std::uint64_t)std::max(m, 1) * sizeof(double);
+}
+
+int frsz2_basis_dot(int dtype, int bits, int block_size, const void* const* basis, int m, uint64_t n,
+                    const void* w, void* h, void* workspace, uint64_t workspace_bytes, void* stream)
+{
+  BasisParams bp{};
+  BasisGeo g{};
+  if (int rc = basis_args(dtype, bits, block_size, basis, m, n, &bp, &g)) return rc;
+  if (m == 0) return FRSZ2_OK;
+  if (!w || !h || !workspace) return set_error(FRSZ2_EFAIL, "null pointer");
+  if (workspace_bytes < frsz2_basis_workspace_size(m, n))
+    return set_error(FRSZ2_EFAIL, "workspace smaller than frsz2_basis_workspace_size()");
+  if (reinterpret_cast<std::uintptr_t>(workspace) % 256 != 0)
+    return set_error(FRSZ2_EFAIL, "workspace must be 256-byte aligned");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (n == 0) return cuda_status(cudaMemsetAsync(h, 0, (std::size_t)m * sizeof(double), s), "memset");
+  int per_sm = 1;
+  switch (bits) {
+#define CASE(B)                                                                                                    \
+  case B: per_sm = dot_ctas_per_sm<B>(); break;
+    FRSZ2_KRYLOV_WIDTHS(CASE)
+#undef CASE
+  }
+  const std::uint64_t chunk = dot_chunk(n, (std::uint64_t)sm_count() * (std::uint64_t)per_sm);
+  const unsigned grid = (unsigned)std::max<std::uint64_t>(1, (n + chunk - 1) / chunk);
+  auto* ticket = static_cast<unsigned int*>(workspace);
+  auto* partials = reinterpret_cast<double*>(static_cast<std::uint8_t*>(workspace) + 256);
+  switch (bits) {
+#define CASE(B)                                                                                                    \
+  case B:                                                                                                          \
+    k_basis_dot<B><<<grid, kKT, 0, s>>>(bp, m, g, static_cast<const double*>(w), chunk, partials, ticket,          \
+                                        static_cast<double*>(h));                                                  \
+    break;
+    FRSZ2_KRYLOV_WIDTHS(CASE)
+#undef CASE
+  }
+  return cuda_status(cudaGetLastError(), "basis dot launch");
+}
+
+int frsz2_basis_axpy(int dtype, int bits, int block_size, const void* const* basis, int m, uint64_t n,
+                     const void* coef, void* y, void* stream)
+{
+  BasisParams bp{};
+  BasisGeo g{};
+  if (int rc = basis_args(dtype, bits, block_size, basis, m, n, &bp, &g)) return rc;
+  if (m == 0 || n == 0) return FRSZ2_OK;
+  if (!coef || !y) return set_error(FRSZ2_EFAIL, "null pointer");
+  if (reinterpret_cast<std::uintptr_t>(y) % 32 != 0) return set_error(FRSZ2_EFAIL, "y must be 32-byte aligned");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const std::uint64_t lanes = (n + 3) / 4;
+  const unsigned grid = (unsigned)std::max<std::uint64_t>(
+    1, std::min<std::uint64_t>((lanes + kKT - 1) / kKT, (std::uint64_t)sm_count() * 8));
+  switch (bits) {
+#define CASE(B)                                                                                                    \
+  case B:                                                                                                          \
+    k_basis_axpy<B><<<grid, kKT, 0, s>>>(bp, m, g, static_cast<const double*>(coef), static_cast<double*>(y));     \
+    break;
+    FRSZ2_KRYLOV_WIDTHS(CASE)
+#undef CASE
+  }
+  return cuda_status(cudaGetLastError(), "basis axpy launch");
+}
+
+} // extern "C"

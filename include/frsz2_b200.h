@@ -154,6 +154,29 @@ void frsz2_batch_destroy(frsz2_batch* plan);
  * stream capture. */
 int frsz2_batch_compress_static(const frsz2_batch_item* items, uint64_t count, void* stream);
 
+/* ---------------------------------------------------------------------------
+ * Decompression fused into its consumer over a compressed basis of m fp64
+ * vectors of n values (the Krylov-basis use of decompress_gpu_element,
+ * include/frsz2.hpp:1096-1104, where a solver reads the basis through the
+ * accessor): values are decoded in registers and fed to the FMAs.  `basis` is a
+ * HOST array of m device pointers to compressed buffers (32-byte aligned), all
+ * with the same bits / block_size / n.  Widths 16, 21, 24, 32, 48, 64; block
+ * sizes that are powers of two without block padding; m <= FRSZ2_MAX_BASIS.
+ *
+ * frsz2_basis_dot:  h[j] = sum_i V_j[i] * w[i], j < m.  `workspace` is device
+ *   memory of frsz2_basis_workspace_size(m, n) bytes, 256-byte aligned, zero
+ *   on first use (the call leaves it ready for the next one); the result does
+ *   not depend on scheduling.  Calls sharing a workspace must not overlap.
+ * frsz2_basis_axpy: y[i] += sum_j c[j] * V_j[i] (j in order), c and y device
+ *   memory, y 32-byte aligned.
+ */
+#define FRSZ2_MAX_BASIS 256
+uint64_t frsz2_basis_workspace_size(int m, uint64_t n);
+int frsz2_basis_dot(int dtype, int bits, int block_size, const void* const* basis, int m, uint64_t n,
+                    const void* w, void* h, void* workspace, uint64_t workspace_bytes, void* stream);
+int frsz2_basis_axpy(int dtype, int bits, int block_size, const void* const* basis, int m, uint64_t n,
+                     const void* coef, void* y, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
