@@ -55,7 +55,7 @@ WORKLOADS = {
     "loguniform_f64_2p25_b16_e64": ("loguniform", "float64", 1 << 25, 16, 64),
 }
 DEFAULT_WORKLOAD = "field512_f32_b16_e32"
-BATCH_WORKLOADS = ("batched4096", "krylov100")
+BATCH_WORKLOADS = ("batched4096", "krylov100", "serving")
 
 # DRAM bytes (read + write) per launch from ncu captures, by (workload, kernel);
 # profiles/ holds the captures' summaries and the commands that made them.
@@ -642,6 +642,94 @@ def run_krylov(args, rank: int, world: int, local_rank: int) -> None:
     print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------------- serving
+
+def run_serving(args, rank: int, world: int, local_rank: int) -> None:
+    """Config 5: a Poisson stream of requests, 60 % compress / 40 % decompress,
+    input sizes log-normal (median 1 MB, sigma 1.5, capped at 256 MB), fp32 /
+    fp64 50/50, bits from {12, 16, 32}, block 32, 32 GB admission budget.
+    Offered load = 70 % of the capacity measured with the same requests all
+    submitted at once.  Latency = completion - arrival, per request."""
+    import torch
+
+    import frsz_b200
+    from frsz_b200 import serve
+
+    torch.cuda.set_device(local_rank)
+    rng = np.random.default_rng(args.seed + rank)
+    pool = []
+    for _ in range(512):  # distinct payloads; requests cycle through them
+        nbytes = min(256 << 20, int(math.exp(rng.normal(math.log(1 << 20), 1.5))))
+        is64 = bool(rng.random() < 0.5)
+        es = 8 if is64 else 4
+        n = max(1, nbytes // es)
+        bits = int(rng.choice([12, 16, 32]))
+        x = torch.randn(n, device="cuda", dtype=torch.float64 if is64 else torch.float32)
+        pool.append(dict(is64=is64, n=n, bits=bits, x=x, comp=frsz_b200.compress(x, bits, 32)))
+    torch.cuda.synchronize()
+    R = args.requests
+    picks = rng.integers(0, len(pool), R)
+    ops = np.where(rng.random(R) < 0.6, serve.OP_COMPRESS, serve.OP_DECOMPRESS)
+
+    def make(count, offsets):
+        """Requests with arrival times relative to their submission."""
+        reqs = (frsz_b200._lib.RequestC * count)()
+        flags = serve.RELEASE_ON_COMPLETION | serve.ARRIVAL_RELATIVE
+        for i in range(count):
+            e = pool[picks[i]]
+            inp = e["x"] if ops[i] == serve.OP_COMPRESS else e["comp"]
+            r = reqs[i]
+            r.op, r.dtype, r.bits, r.block_size, r.n = int(ops[i]), int(e["is64"]), e["bits"], 32, e["n"]
+            r.input, r.output, r.arrival_ns, r.flags = inp.data_ptr(), None, int(offsets[i]), flags
+        return reqs
+
+    def drive(reqs, count):
+        sv = serve.Server(memory_budget=32 << 30, max_batch=args.max_batch, streams=args.streams)
+        sv.submit(reqs)
+        got = []
+        while len(got) < count:
+            got += sv.poll(wait_ms=50)
+        st = sv.stats()
+        sv.close()
+        assert all(c.status == 0 for c in got), "a serving request failed"
+        return got, st
+
+    # warm-up: loads every class kernel the stream uses (lazy module loading)
+    drive(make(min(R, 2000), np.zeros(min(R, 2000))), min(R, 2000))
+    # capacity: every request arrives at submission
+    cap_n = min(R, args.capacity_requests)
+    got, _ = drive(make(cap_n, np.zeros(cap_n)), cap_n)
+    span = (max(c.done_ns for c in got) - min(c.arrival_ns for c in got)) / 1e9
+    cap_bytes = sum(c.bytes for c in got) / span
+    cap_rate = cap_n / span
+    # Poisson stream at `load` of that capacity, starting 20 ms after submission
+    lam = args.load * cap_rate
+    offsets = 20_000_000 + np.cumsum(rng.exponential(1e9 / lam, R)).astype(np.int64)
+    got, st = drive(make(R, offsets), R)
+    lat = np.array([c.latency_ns for c in got], dtype=np.float64) / 1e3
+    total = sum(c.bytes for c in got)
+    span = (max(c.done_ns for c in got) - min(c.arrival_ns for c in got)) / 1e9
+    if rank != 0:
+        return
+    line = {
+        "metric": METRIC, "value": round(world * total / span / 1e9, 3), "unit": "GB/s", "n_gpus": world,
+        "steps": R, "warmup": 0, "ms_per_step": round(span * 1e3 / R, 5), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u32/u64", "data": "synthetic",
+        "config": {"workload": "serving", "requests": R, "compress_fraction": 0.6,
+                   "sizes": "log-normal median 1 MB sigma 1.5, cap 256 MB", "dtypes": "fp32/fp64 50/50",
+                   "bits": [12, 16, 32], "block_size": 32, "budget_bytes": 32 << 30, "load": args.load,
+                   "max_batch": args.max_batch, "streams": args.streams},
+        "latency_us": {"p50": round(float(np.percentile(lat, 50)), 1), "p90": round(float(np.percentile(lat, 90)), 1),
+                       "p99": round(float(np.percentile(lat, 99)), 1),
+                       "p999": round(float(np.percentile(lat, 99.9)), 1), "max": round(float(lat.max()), 1)},
+        "capacity": {"gbs": round(cap_bytes / 1e9, 1), "requests_per_s": round(cap_rate, 1),
+                     "requests": cap_n},
+        "offered_requests_per_s": round(lam, 1),
+        "server": st,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
     ap.add_argument("--gpus", type=int, default=1)
@@ -654,6 +742,11 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=3.0)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--requests", type=int, default=100_000, help="serving: requests in the Poisson stream")
+    ap.add_argument("--capacity-requests", type=int, default=20_000, help="serving: requests of the capacity probe")
+    ap.add_argument("--load", type=float, default=0.7, help="serving: offered load as a fraction of capacity")
+    ap.add_argument("--max-batch", type=int, default=256)
+    ap.add_argument("--streams", type=int, default=4)
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     rank = int(os.environ.get("RANK", "0"))
@@ -663,6 +756,8 @@ def main():
         run_batched(args, rank, world, local_rank)
     elif args.workload == "krylov100":
         run_krylov(args, rank, world, local_rank)
+    elif args.workload == "serving":
+        run_serving(args, rank, world, local_rank)
     elif args.impl == "reference":
         run_reference_arm(args, rank, world)
     else:

@@ -23,6 +23,7 @@ from .codec import (
 from .plugin import Frsz2Plugin
 from .batch import BatchArray, BatchPlan
 from .krylov import CompressedBasis
+from . import serve
 
 __all__ = [
     "FRSZ2_DOUBLE", "FRSZ2_EDTYPE", "FRSZ2_EFAIL", "FRSZ2_FLOAT", "FRSZ2_OK", "Frsz2Error", "lib",

@@ -38,6 +38,27 @@ class BatchStatsC(ctypes.Structure):
                 ("side_by_side", ctypes.c_int * 2), ("tuned", ctypes.c_int * 2)]
 
 
+class RequestC(ctypes.Structure):
+    """frsz2_request (include/frsz2_b200.h)."""
+    _fields_ = [("op", ctypes.c_int), ("dtype", ctypes.c_int), ("bits", ctypes.c_int), ("block_size", ctypes.c_int),
+                ("n", ctypes.c_uint64), ("input", ctypes.c_void_p), ("output", ctypes.c_void_p),
+                ("arrival_ns", ctypes.c_uint64), ("flags", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
+
+
+class CompletionC(ctypes.Structure):
+    """frsz2_completion (include/frsz2_b200.h)."""
+    _fields_ = [("id", ctypes.c_uint64), ("status", ctypes.c_int), ("op", ctypes.c_int), ("output", ctypes.c_void_p),
+                ("output_bytes", ctypes.c_uint64), ("bytes", ctypes.c_uint64), ("arrival_ns", ctypes.c_uint64),
+                ("admit_ns", ctypes.c_uint64), ("done_ns", ctypes.c_uint64)]
+
+
+class CountersC(ctypes.Structure):
+    """frsz2_server_counters (include/frsz2_b200.h)."""
+    _fields_ = [(k, ctypes.c_uint64) for k in ("completed", "failed", "batches", "bytes", "pending", "budget_bytes",
+                                               "arena_used_bytes", "arena_peak_bytes", "max_batch",
+                                               "max_inflight_output_bytes")]
+
+
 # name -> (restype, argtypes); kept in step with include/frsz2_b200.h
 SIGNATURES = {
     "register_frsz": (None, []),
@@ -50,6 +71,8 @@ SIGNATURES = {
     "frsz2_compress_host": (_int, [_int, _int, _int, _vp, _u64, _vp, _vp]),
     "frsz2_decompress_host": (_int, [_int, _int, _int, _vp, _u64, _vp, _vp]),
     "frsz2_decompress_elements": (_int, [_int, _int, _int, _vp, _u64, _vp, _u64, _vp, _vp]),
+    "frsz2_compress_blocks": (_int, [_int, _int, _int, _vp, _u64, _u64, _u64, _vp, _vp]),
+    "frsz2_decompress_blocks": (_int, [_int, _int, _int, _vp, _u64, _u64, _u64, _vp, _vp]),
     "frsz2_batch_create": (_int, [ctypes.POINTER(BatchItemC), _u64, ctypes.POINTER(_vp)]),
     "frsz2_batch_compress": (_int, [_vp, _vp]),
     "frsz2_batch_decompress": (_int, [_vp, _vp]),
@@ -60,6 +83,14 @@ SIGNATURES = {
     "frsz2_basis_workspace_size": (_u64, [_int, _u64]),
     "frsz2_basis_dot": (_int, [_int, _int, _int, ctypes.POINTER(_vp), _int, _u64, _vp, _vp, _vp, _u64, _vp]),
     "frsz2_basis_axpy": (_int, [_int, _int, _int, ctypes.POINTER(_vp), _int, _u64, _vp, _vp, _vp]),
+    "frsz2_now_ns": (_u64, []),
+    "frsz2_server_create": (_int, [_u64, _int, _int, ctypes.POINTER(_vp)]),
+    "frsz2_server_submit": (_int, [_vp, ctypes.POINTER(RequestC), _u64, ctypes.POINTER(_u64)]),
+    "frsz2_server_cancel": (_int, [_vp, _u64]),
+    "frsz2_server_poll": (_int, [_vp, ctypes.POINTER(CompletionC), _u64, ctypes.POINTER(_u64), _int]),
+    "frsz2_server_release": (_int, [_vp, _u64]),
+    "frsz2_server_stats": (_int, [_vp, ctypes.POINTER(CountersC)]),
+    "frsz2_server_destroy": (None, [_vp]),
 }
 
 

@@ -406,6 +406,45 @@ int frsz2_decompress_host(int dtype, int bits, int block_size, const void* h_com
   return host_codec(false, dtype, bits, block_size, h_compressed, n, h_values, static_cast<cudaStream_t>(stream));
 }
 
+static int block_range_args(int dtype, int bits, int E, std::uint64_t n, std::uint64_t b0, std::uint64_t count,
+                            const void* values, const void* buf, Layout* L)
+{
+  if (int rc = check_args(dtype, bits, E)) return rc;
+  *L = make_layout(n, bits, E);
+  if (b0 > L->nb || count > L->nb - b0) return set_error(FRSZ2_EFAIL, "block range outside the array");
+  if (count == 0) return FRSZ2_OK;
+  if (!values || !buf) return set_error(FRSZ2_EFAIL, "null pointer");
+  return check_alignment(dtype, *L, values, buf);
+}
+
+int frsz2_compress_blocks(int dtype, int bits, int block_size, const void* d_values, uint64_t n, uint64_t block_begin,
+                          uint64_t block_count, void* d_compressed, void* stream)
+{
+  Layout L;
+  if (int rc = block_range_args(dtype, bits, block_size, n, block_begin, block_count, d_values, d_compressed, &L))
+    return rc;
+  if (block_count == 0) return FRSZ2_OK;
+  // job_for_slice offsets the value pointer by the range's first value itself
+  const std::size_t es = dtype == FRSZ2_FLOAT ? 4 : 8;
+  const void* base = static_cast<const std::uint8_t*>(d_values) - block_begin * (std::uint64_t)block_size * es;
+  Job j = job_for_slice(L, dtype, block_begin, block_count, base, nullptr, static_cast<std::uint8_t*>(d_compressed));
+  return launch_compress(j, dtype, static_cast<cudaStream_t>(stream), nullptr);
+}
+
+int frsz2_decompress_blocks(int dtype, int bits, int block_size, const void* d_compressed, uint64_t n,
+                            uint64_t block_begin, uint64_t block_count, void* d_values, void* stream)
+{
+  Layout L;
+  if (int rc = block_range_args(dtype, bits, block_size, n, block_begin, block_count, d_values, d_compressed, &L))
+    return rc;
+  if (block_count == 0) return FRSZ2_OK;
+  const std::size_t es = dtype == FRSZ2_FLOAT ? 4 : 8;
+  void* base = static_cast<std::uint8_t*>(d_values) - block_begin * (std::uint64_t)block_size * es;
+  Job j = job_for_slice(L, dtype, block_begin, block_count, nullptr, base,
+                        const_cast<std::uint8_t*>(static_cast<const std::uint8_t*>(d_compressed)));
+  return launch_decompress(j, dtype, static_cast<cudaStream_t>(stream), nullptr);
+}
+
 int frsz2_decompress_elements(int dtype, int bits, int block_size, const void* d_compressed, uint64_t n,
                               const uint64_t* d_idx, uint64_t count, void* d_out, void* stream)
 {

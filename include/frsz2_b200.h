@@ -85,6 +85,18 @@ int frsz2_compress_host(int dtype, int bits, int block_size, const void* h_value
 int frsz2_decompress_host(int dtype, int bits, int block_size, const void* h_compressed, uint64_t n, void* h_values,
                           void* stream);
 
+/* Blocks [block_begin, block_begin + block_count) of an array of n values,
+ * written into / read from the WHOLE array's compressed buffer `d_compressed`
+ * (its own exponent slots and block words, nothing else).  `d_values` points at
+ * the value of the first block (block_begin * block_size).  The range analogue
+ * of compress_cpu_block / decompress_cpu_block (include/frsz2.hpp:1108-1179,
+ * 1217-1240): ranks or streams that own disjoint block ranges of one array can
+ * work on it independently. */
+int frsz2_compress_blocks(int dtype, int bits, int block_size, const void* d_values, uint64_t n, uint64_t block_begin,
+                          uint64_t block_count, void* d_compressed, void* stream);
+int frsz2_decompress_blocks(int dtype, int bits, int block_size, const void* d_compressed, uint64_t n,
+                            uint64_t block_begin, uint64_t block_count, void* d_values, void* stream);
+
 /* Random-access decode of `count` elements at device indices d_idx[0..count)
  * into d_out.  Replaces decompress_gpu_element (include/frsz2.hpp:1096-1104)
  * and decompress_cpu_element (include/frsz2.hpp:1199-1214); values are
@@ -176,6 +188,68 @@ int frsz2_basis_dot(int dtype, int bits, int block_size, const void* const* basi
                     const void* w, void* h, void* workspace, uint64_t workspace_bytes, void* stream);
 int frsz2_basis_axpy(int dtype, int bits, int block_size, const void* const* basis, int m, uint64_t n,
                      const void* coef, void* y, void* stream);
+
+/* ---------------------------------------------------------------------------
+ * Request server: no counterpart in the reference.  Compress / decompress
+ * requests of any size arrive over time (arrival_ns, CLOCK_MONOTONIC as
+ * returned by frsz2_now_ns; 0 = at submission).  A worker thread admits
+ * eligible requests in arrival order into batches -- skipping, within a
+ * bounded window, requests whose output does not fit the memory budget right
+ * now -- and launches each batch on a free stream as soon as one exists, so
+ * requests that arrive while others run overlap with them on the device.
+ * Outputs go to the caller's `output` or, when it is NULL, to the server's
+ * arena of `memory_budget` bytes, where they stay until frsz2_server_release
+ * (or until completion with FRSZ2_REQ_RELEASE_ON_COMPLETION).  A request's
+ * result is the same as a plain frsz2_compress / frsz2_decompress of it.
+ * Completion statuses: 0 ok, 1 / 2 as elsewhere (including "request output
+ * larger than the server's memory budget"), 3 cancelled before admission.
+ */
+#define FRSZ2_ECANCELLED 3
+#define FRSZ2_OP_COMPRESS 0
+#define FRSZ2_OP_DECOMPRESS 1
+#define FRSZ2_REQ_RELEASE_ON_COMPLETION 1u
+#define FRSZ2_REQ_ARRIVAL_RELATIVE 2u /* arrival_ns is an offset from the submit call */
+
+typedef struct frsz2_server frsz2_server;
+
+typedef struct frsz2_request {
+  int op;               /* FRSZ2_OP_COMPRESS / FRSZ2_OP_DECOMPRESS */
+  int dtype;
+  int bits;
+  int block_size;
+  uint64_t n;           /* values */
+  const void* input;    /* device: values (compress) or compressed buffer (decompress) */
+  void* output;         /* device, or NULL to allocate from the server's arena */
+  uint64_t arrival_ns;  /* eligible from this time on; 0 = at submission */
+  uint32_t flags;       /* FRSZ2_REQ_* */
+  uint32_t reserved;
+} frsz2_request;
+
+typedef struct frsz2_completion {
+  uint64_t id;
+  int status;
+  int op;
+  void* output;          /* where the result is */
+  uint64_t output_bytes; /* arena bytes held until released (0 if none) */
+  uint64_t bytes;        /* algorithmic bytes moved */
+  uint64_t arrival_ns, admit_ns, done_ns;
+} frsz2_completion;
+
+typedef struct frsz2_server_counters {
+  uint64_t completed, failed, batches, bytes, pending;
+  uint64_t budget_bytes, arena_used_bytes, arena_peak_bytes;
+  uint64_t max_batch, max_inflight_output_bytes;
+} frsz2_server_counters;
+
+uint64_t frsz2_now_ns(void);
+int frsz2_server_create(uint64_t memory_budget, int max_batch, int streams, frsz2_server** server);
+int frsz2_server_submit(frsz2_server* server, const frsz2_request* requests, uint64_t count, uint64_t* first_id);
+int frsz2_server_cancel(frsz2_server* server, uint64_t id);
+/* Up to `max` completions; waits up to wait_ms for the first one. */
+int frsz2_server_poll(frsz2_server* server, frsz2_completion* out, uint64_t max, uint64_t* count, int wait_ms);
+int frsz2_server_release(frsz2_server* server, uint64_t id);
+int frsz2_server_stats(frsz2_server* server, frsz2_server_counters* stats);
+void frsz2_server_destroy(frsz2_server* server);
 
 #ifdef __cplusplus
 }

@@ -83,6 +83,23 @@ def oracle_lib():
     return _oracle
 
 
+REF_GPU_SO = os.path.join(HERE, "_ref", "libfrsz2_ref_gpu.so")
+_ref_gpu = None
+
+
+def ref_gpu_lib():
+    """The reference's own GPU kernels (compress_gpu / decompress_gpu) for the
+    benchmark configurations; speed bar only, not the oracle."""
+    global _ref_gpu
+    if _ref_gpu is None:
+        if not os.path.exists(REF_GPU_SO):
+            raise FileNotFoundError(f"{REF_GPU_SO} not built (needs the reference sources; see oracle/Makefile)")
+        lib = ctypes.CDLL(REF_GPU_SO)
+        lib.frsz2ref_gpu.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp, _c_size, _vp, _vp]
+        _ref_gpu = lib
+    return _ref_gpu
+
+
 def ref_available() -> bool:
     return os.path.exists(REF_SO)
 
