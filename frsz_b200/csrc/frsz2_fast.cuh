@@ -612,9 +612,12 @@ namespace frsz2b {
 template<class T, int BITS>
 struct lane_words
 {
-  std::uint32_t w[fast_cfg<T, BITS>::NW + 1];
-  std::int64_t be;
-  int o; // bit offset of the segment in w[0]
+  using Cfg = fast_cfg<T, BITS>;
+  // 32-bit exponents for W <= 32 keep the record small; only W = 64 needs more
+  using exp_t = std::conditional_t<(Cfg::W == 64), std::int64_t, std::int32_t>;
+  std::uint32_t w[Cfg::ALIGNED ? Cfg::NW : Cfg::NW + 1];
+  exp_t be;
+  int o; // bit offset of the segment in w[0] (unaligned widths only)
 };
 
 template<class T, int BITS>
@@ -624,7 +627,7 @@ __device__ __forceinline__ void fast_load_lane(const std::uint8_t* __restrict__ 
 {
   using Cfg = fast_cfg<T, BITS>;
   constexpr int L = Cfg::L, NW = Cfg::NW, W = Cfg::W;
-  lw.be = load_exp(exps + (idx >> log2E) * (std::uint64_t)(W / 8), W);
+  lw.be = (typename lane_words<T, BITS>::exp_t)load_exp(exps + (idx >> log2E) * (std::uint64_t)(W / 8), W);
   const std::uint64_t S = idx * (std::uint64_t)BITS;
   const std::uint32_t* src = reinterpret_cast<const std::uint32_t*>(words) + (S >> 5);
   lw.o = (int)(S & 31u);
@@ -633,7 +636,6 @@ __device__ __forceinline__ void fast_load_lane(const std::uint8_t* __restrict__ 
     load_words<NW>(src, t);
 #pragma unroll
     for (int i = 0; i < NW; ++i) lw.w[i] = t[i];
-    lw.w[NW] = 0;
   } else {
 #pragma unroll
     for (int i = 0; i < NW; ++i) lw.w[i] = __ldg(src + i);
@@ -651,7 +653,8 @@ __device__ __forceinline__ void fast_decode_loaded(const lane_words<T, BITS>& lw
   std::uint32_t seg[NW + 1];
   if constexpr (Cfg::ALIGNED) {
 #pragma unroll
-    for (int i = 0; i <= NW; ++i) seg[i] = lw.w[i];
+    for (int i = 0; i < NW; ++i) seg[i] = lw.w[i];
+    seg[NW] = 0;
   } else {
 #pragma unroll
     for (int i = 0; i < NW; ++i) seg[i] = __funnelshift_r(lw.w[i], lw.w[i + 1], lw.o);

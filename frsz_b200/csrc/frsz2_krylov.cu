@@ -27,7 +27,14 @@ namespace {
 constexpr int kMaxBasis = FRSZ2_MAX_BASIS;
 constexpr int kKT = 256;            // threads per CTA
 constexpr int kSub = 3072;          // w values staged per step (24 KiB)
-constexpr int kJB = 8;              // basis vectors whose loads are in flight together
+#ifndef FRSZ2_KRYLOV_JB
+#define FRSZ2_KRYLOV_JB 4
+#endif
+#ifndef FRSZ2_KRYLOV_MIN_CTAS
+#define FRSZ2_KRYLOV_MIN_CTAS 4
+#endif
+constexpr int kJB = FRSZ2_KRYLOV_JB;             // basis vectors whose loads are in flight together
+constexpr int kMinCtas = FRSZ2_KRYLOV_MIN_CTAS; // resident CTAs per SM the register budget must allow
 
 struct BasisParams
 {
@@ -42,7 +49,7 @@ struct BasisGeo
 };
 
 template<int BITS>
-__global__ void __launch_bounds__(kKT)
+__global__ void __launch_bounds__(kKT, kMinCtas)
   k_basis_dot(const __grid_constant__ BasisParams bp, int m, BasisGeo g, const double* __restrict__ w,
               std::uint64_t chunk, double* __restrict__ partials, unsigned int* __restrict__ ticket,
               double* __restrict__ h)
@@ -118,7 +125,7 @@ __global__ void __launch_bounds__(kKT)
 }
 
 template<int BITS>
-__global__ void __launch_bounds__(kKT)
+__global__ void __launch_bounds__(kKT, kMinCtas)
   k_basis_axpy(const __grid_constant__ BasisParams bp, int m, BasisGeo g, const double* __restrict__ coef,
                double* __restrict__ y)
 {
