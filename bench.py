@@ -471,8 +471,8 @@ def run_batched(args, rank: int, world: int, local_rank: int) -> None:
     stream = torch.cuda.Stream()  # graph capture needs a non-default stream
     torch.cuda.set_stream(stream)
     plan = frsz_b200.BatchPlan(arrays)
-    tune_c = plan.autotune(compress=True, stream=stream)
-    tune_d = plan.autotune(compress=False, stream=stream)
+    tune_c = plan.autotune(compress=True, stream=stream) if args.batch_autotune else None
+    tune_d = plan.autotune(compress=False, stream=stream) if args.batch_autotune else None
 
     def timed(fn, k):
         for _ in range(args.warmup):
@@ -548,7 +548,8 @@ def run_batched(args, rank: int, world: int, local_rank: int) -> None:
         "batched": {"compress_gbs": round(total_bytes / ms_c / 1e6, 1),
                     "decompress_gbs": round(total_bytes / ms_d / 1e6, 1),
                     "hbm_frac": round(2 * total_bytes / step_ms / 1e6 / peaks["hbm_gbs"], 4),
-                    "autotune_ms": {"compress": round(tune_c, 4), "decompress": round(tune_d, 4)},
+                    "autotune_ms": ({"compress": round(tune_c, 4), "decompress": round(tune_d, 4)}
+                                    if args.batch_autotune else None),
                     "plan": info},
         "per_array_plain": {"gbs": round(2 * total_bytes / per_ms / 1e6, 1), "ms_per_step": round(per_ms, 3),
                             "launches_per_step": 2 * len(arrays), "host_loop": "python ctypes"},
@@ -571,7 +572,7 @@ def run_krylov(args, rank: int, world: int, local_rank: int) -> None:
     import frsz_b200
 
     torch.cuda.set_device(local_rank)
-    m, n, bits, E = 100, 1 << 22, 32, 32
+    m, n, bits, E = args.krylov_vectors, 1 << 22, 32, 32
     g = torch.Generator(device="cuda").manual_seed(args.seed + rank)
     V = torch.randn(m, n, generator=g, device="cuda", dtype=torch.float64)
     basis = frsz_b200.CompressedBasis(m, n, bits=bits, block_size=E)
@@ -626,7 +627,8 @@ def run_krylov(args, rank: int, world: int, local_rank: int) -> None:
         "metric": METRIC, "value": round(value, 3), "unit": "GB/s", "n_gpus": world, "steps": K,
         "warmup": args.warmup, "ms_per_step": round(ms_dot + ms_axpy, 4), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": "krylov100", "vectors": m, "n": n, "bits": bits, "block_size": E,
+        "config": {"workload": "krylov100" if m == 100 else f"krylov{m}", "vectors": m, "n": n, "bits": bits,
+                   "block_size": E,
                    "compressed_basis_bytes": comp_bytes, "step": "fused dot h=V^T w, then fused axpy y+=V c"},
         "fused_dot": {"ms": round(ms_dot, 4), "gbs": round(dot_bytes / ms_dot / 1e6, 1),
                       "hbm_frac": round(dot_bytes / ms_dot / 1e6 / peaks["hbm_gbs"], 4), "max_rel_err": dot_err},
@@ -746,6 +748,9 @@ def main():
     ap.add_argument("--capacity-requests", type=int, default=20_000, help="serving: requests of the capacity probe")
     ap.add_argument("--load", type=float, default=0.7, help="serving: offered load as a fraction of capacity")
     ap.add_argument("--max-batch", type=int, default=256)
+    ap.add_argument("--no-batch-autotune", dest="batch_autotune", action="store_false",
+                    help="batched4096: keep the plan's default launch shape")
+    ap.add_argument("--krylov-vectors", type=int, default=100, help="krylov100: basis size")
     ap.add_argument("--streams", type=int, default=4)
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
