@@ -135,6 +135,34 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
+# ---------------------------------------------------------------- accuracy
+
+def error_report(x, y, buf, bits: int, E: int) -> dict:
+    """Max |x - x_hat|, max |x - x_hat| / |x| over nonzero x (both against the
+    fp64 value of the input) and the number of values outside the per-block
+    bound max(2^(e_b - bits + 2), 2^(e_b - 31)) that truncation guarantees."""
+    import torch
+
+    n = x.numel()
+    w = 8 if bits <= 8 else 16 if bits <= 16 else 32 if bits <= 32 else 64
+    nb = -(-n // E)
+    exps = buf[: nb * (w // 8)].view({8: torch.int8, 16: torch.int16, 32: torch.int32, 64: torch.int64}[w])
+    exps = exps.to(torch.float64)
+    bound = torch.maximum(torch.exp2(exps - bits + 2), torch.exp2(exps - 31))
+    max_abs, max_rel, bad = 0.0, 0.0, 0
+    chunk = (1 << 24) // E * E
+    for s0 in range(0, n, chunk):
+        xe = x[s0:s0 + chunk].to(torch.float64)
+        err = (xe - y[s0:s0 + chunk].to(torch.float64)).abs()
+        b = bound[s0 // E:(s0 + xe.numel() + E - 1) // E].repeat_interleave(E)[: xe.numel()]
+        bad += int((err > b).sum())
+        max_abs = max(max_abs, float(err.max()))
+        nz = xe != 0
+        if bool(nz.any()):
+            max_rel = max(max_rel, float((err[nz] / xe[nz].abs()).max()))
+    return {"max_abs": max_abs, "max_rel": max_rel, "bound_violations": bad, "against": "fp64 of the input"}
+
+
 # ---------------------------------------------------------------- inputs
 
 def make_input_cuda(kind: str, dtype: str, n: int, seed: int):
@@ -334,6 +362,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
         comp_avg, decomp_avg = statistics.mean(comp_ms), statistics.mean(decomp_ms)
 
     value = world * step_bytes * K / (elapsed_ms / 1e3) / 1e9
+    errors = error_report(x, y, buf, bits, E)
 
     # ---- end to end through the host-buffer C ABI
     e2e = None
@@ -409,6 +438,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 2), "peak": peaks["hbm_gbs"],
                      "unit": "GB/s", "frac": round(achieved / peaks["hbm_gbs"], 4), "traffic": traffic,
                      "algorithmic_bytes": per_launch, "peak_source": peaks["source"]},
+        "errors": errors,
         "cpu_baseline": cpu,
         "e2e": e2e,
         "gpu_launches": 2 * K,

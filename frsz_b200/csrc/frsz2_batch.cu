@@ -333,18 +333,21 @@ int frsz2_batch_create(const frsz2_batch_item* items, uint64_t count, frsz2_batc
 
 int frsz2_batch_compress(frsz2_batch* plan, void* stream)
 {
+  NvtxRange nvtx("frsz2_batch_compress");
   if (!plan) return set_error(FRSZ2_EFAIL, "null plan");
   return run(plan, true, static_cast<cudaStream_t>(stream));
 }
 
 int frsz2_batch_decompress(frsz2_batch* plan, void* stream)
 {
+  NvtxRange nvtx("frsz2_batch_decompress");
   if (!plan) return set_error(FRSZ2_EFAIL, "null plan");
   return run(plan, false, static_cast<cudaStream_t>(stream));
 }
 
 int frsz2_batch_autotune(frsz2_batch* plan, int compress, void* stream, float* best_ms)
 {
+  NvtxRange nvtx("frsz2_batch_autotune");
   if (!plan) return set_error(FRSZ2_EFAIL, "null plan");
   std::lock_guard<std::mutex> lock(plan->mu);
   if (int rc = check_direction(plan, compress != 0)) return rc;

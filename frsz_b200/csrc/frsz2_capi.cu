@@ -370,6 +370,7 @@ int frsz2_exponent_size(int dtype, int bits, int block_size, uint64_t n, uint64_
 int frsz2_compress(int dtype, int bits, int block_size, const void* d_values, uint64_t n, void* d_compressed,
                    void* stream)
 {
+  NvtxRange nvtx("frsz2_compress");
   int rc = check_args(dtype, bits, block_size);
   if (rc) return rc;
   if (n == 0) return FRSZ2_OK;
@@ -383,6 +384,7 @@ int frsz2_compress(int dtype, int bits, int block_size, const void* d_values, ui
 int frsz2_decompress(int dtype, int bits, int block_size, const void* d_compressed, uint64_t n, void* d_values,
                      void* stream)
 {
+  NvtxRange nvtx("frsz2_decompress");
   int rc = check_args(dtype, bits, block_size);
   if (rc) return rc;
   if (n == 0) return FRSZ2_OK;
@@ -397,12 +399,14 @@ int frsz2_decompress(int dtype, int bits, int block_size, const void* d_compress
 int frsz2_compress_host(int dtype, int bits, int block_size, const void* h_values, uint64_t n, void* h_compressed,
                         void* stream)
 {
+  NvtxRange nvtx("frsz2_compress_host");
   return host_codec(true, dtype, bits, block_size, h_values, n, h_compressed, static_cast<cudaStream_t>(stream));
 }
 
 int frsz2_decompress_host(int dtype, int bits, int block_size, const void* h_compressed, uint64_t n, void* h_values,
                           void* stream)
 {
+  NvtxRange nvtx("frsz2_decompress_host");
   return host_codec(false, dtype, bits, block_size, h_compressed, n, h_values, static_cast<cudaStream_t>(stream));
 }
 
@@ -420,6 +424,7 @@ static int block_range_args(int dtype, int bits, int E, std::uint64_t n, std::ui
 int frsz2_compress_blocks(int dtype, int bits, int block_size, const void* d_values, uint64_t n, uint64_t block_begin,
                           uint64_t block_count, void* d_compressed, void* stream)
 {
+  NvtxRange nvtx("frsz2_compress_blocks");
   Layout L;
   if (int rc = block_range_args(dtype, bits, block_size, n, block_begin, block_count, d_values, d_compressed, &L))
     return rc;
@@ -434,6 +439,7 @@ int frsz2_compress_blocks(int dtype, int bits, int block_size, const void* d_val
 int frsz2_decompress_blocks(int dtype, int bits, int block_size, const void* d_compressed, uint64_t n,
                             uint64_t block_begin, uint64_t block_count, void* d_values, void* stream)
 {
+  NvtxRange nvtx("frsz2_decompress_blocks");
   Layout L;
   if (int rc = block_range_args(dtype, bits, block_size, n, block_begin, block_count, d_values, d_compressed, &L))
     return rc;
@@ -448,6 +454,7 @@ int frsz2_decompress_blocks(int dtype, int bits, int block_size, const void* d_c
 int frsz2_decompress_elements(int dtype, int bits, int block_size, const void* d_compressed, uint64_t n,
                               const uint64_t* d_idx, uint64_t count, void* d_out, void* stream)
 {
+  NvtxRange nvtx("frsz2_decompress_elements");
   int rc = check_args(dtype, bits, block_size);
   if (rc) return rc;
   if (count == 0) return FRSZ2_OK;

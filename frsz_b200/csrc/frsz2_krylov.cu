@@ -249,6 +249,7 @@ uint64_t frsz2_basis_workspace_size(int m, uint64_t n)
 int frsz2_basis_dot(int dtype, int bits, int block_size, const void* const* basis, int m, uint64_t n,
                     const void* w, void* h, void* workspace, uint64_t workspace_bytes, void* stream)
 {
+  NvtxRange nvtx("frsz2_basis_dot");
   BasisParams bp{};
   BasisGeo g{};
   if (int rc = basis_args(dtype, bits, block_size, basis, m, n, &bp, &g)) return rc;
@@ -286,6 +287,7 @@ int frsz2_basis_dot(int dtype, int bits, int block_size, const void* const* basi
 int frsz2_basis_axpy(int dtype, int bits, int block_size, const void* const* basis, int m, uint64_t n,
                      const void* coef, void* y, void* stream)
 {
+  NvtxRange nvtx("frsz2_basis_axpy");
   BasisParams bp{};
   BasisGeo g{};
   if (int rc = basis_args(dtype, bits, block_size, basis, m, n, &bp, &g)) return rc;

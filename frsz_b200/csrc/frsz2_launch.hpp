@@ -7,6 +7,7 @@
 #include <string>
 
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 namespace frsz2b {
 
@@ -21,6 +22,16 @@ int cuda_status(cudaError_t e, const char* what);
 int check_args(int dtype, int bits, int E);
 
 int sm_count();
+
+// NVTX range around a C-ABI call (visible in nsys / ncu timelines; a no-op
+// without a tool attached).
+struct NvtxRange
+{
+  explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange&) = delete;
+  NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 Job make_job(const Layout& L, int dtype);
 bool tile_eligible(const Job& j, int dtype, const void* values, const void* words);

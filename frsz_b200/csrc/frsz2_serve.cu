@@ -171,6 +171,7 @@ int validate(const frsz2_request& r, std::uint64_t budget)
 // Launch one admitted batch on slot s.
 int launch_batch(frsz2_server* sv, Slot& s)
 {
+  NvtxRange nvtx("frsz2_server batch");
   std::uint64_t per_key[kKeys] = {};
   auto key = [](const Req* q) {
     return (q->r.op == FRSZ2_OP_COMPRESS ? 130 : 0) + (q->r.dtype == FRSZ2_DOUBLE ? 65 : 0) + q->r.bits;
