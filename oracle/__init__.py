@@ -12,6 +12,10 @@ Two libraries, both built by ``oracle/Makefile``:
 * ``_ref/libfrsz2_ref.so`` -- the reference's own ``frsz2.hpp`` compiled
   unmodified behind ``ref_shim.cpp``.  Present where it was built (it travels
   with the repository snapshot as a git-ignored binary).
+* ``_ref/libfrsz2_ref_gpu.so`` -- the reference's own GPU kernels
+  (``compress_gpu`` / ``decompress_gpu``) behind ``ref_gpu_shim.cu``, a speed bar
+  for the GPU tests (not a checker: their zero-code decode differs from the
+  reference CPU codec).
 """
 from __future__ import annotations
 
