@@ -160,7 +160,13 @@ def error_report(x, y, buf, bits: int, E: int) -> dict:
         nz = xe != 0
         if bool(nz.any()):
             max_rel = max(max_rel, float((err[nz] / xe[nz].abs()).max()))
-    return {"max_abs": max_abs, "max_rel": max_rel, "bound_violations": bad, "against": "fp64 of the input"}
+    out = {"max_abs": max_abs, "max_rel": max_rel, "bound_violations": bad, "against": "fp64 of the input"}
+    if not math.isfinite(max_rel):
+        # a value ~2^-1000 in a block whose maximum is ~2^+1000 decodes to the
+        # block's zero level; the ratio overflows fp64 (strict JSON has no Inf)
+        out["max_rel"] = None
+        out["max_rel_note"] = "overflows fp64 (values far below their block maximum)"
+    return out
 
 
 # ---------------------------------------------------------------- inputs

@@ -23,13 +23,14 @@ __global__ void __launch_bounds__(NT)
   k_batch_class(const BatchItem* __restrict__ items, int nitems, std::uint64_t total_tiles)
 {
   __shared__ std::uint32_t s_rmax[2 * (NT / 32) * RPW];
+  __shared__ __align__(16) std::uint32_t s_stage[stage_words<T, BITS, NT, RPW>::value];
   int cur = 0;
   for (std::uint64_t t = blockIdx.x; t < total_tiles; t += gridDim.x) {
     while (cur + 1 < nitems && items[cur + 1].tile_begin <= t) ++cur;
     const Job j = items[cur].job;
     const std::uint64_t lt = t - items[cur].tile_begin;
     if (COMPRESS)
-      fast_compress_tile<T, BITS, NT, RPW>(j, lt, s_rmax);
+      fast_compress_tile<T, BITS, NT, RPW>(j, lt, s_rmax, s_stage);
     else
       fast_decompress_tile<T, BITS, NT, RPW>(j, lt);
   }

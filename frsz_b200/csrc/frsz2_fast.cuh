@@ -290,10 +290,25 @@ __device__ __forceinline__ typename fp<T>::U decode_plain(typename fast_cfg<T, B
 
 // ---------------------------------------------------------------- compress
 
+#ifndef FRSZ2_STAGE_UNALIGNED_ROWS
+#define FRSZ2_STAGE_UNALIGNED_ROWS 1
+#endif
+
+// Shared-memory words a CTA needs to stage its warps' packed rows (only the
+// unaligned widths stage; one row of L words per warp, 16-byte aligned).
+template<class T, int BITS, int NT, int RPW>
+struct stage_words
+{
+  using Cfg = fast_cfg<T, BITS, NT, RPW>;
+  static constexpr int value = (!Cfg::ALIGNED && FRSZ2_STAGE_UNALIGNED_ROWS) ? Cfg::WARPS * Cfg::L : 4;
+};
+
 // One tile of compress.  s_rmax: 2 * Cfg::ROWS words of shared memory (used
-// only when an exponent block spans several warp rows).
+// only when an exponent block spans several warp rows); s_stage:
+// stage_words<>::value words, 16-byte aligned.
 template<class T, int BITS, int NT, int RPW_>
-__device__ __forceinline__ void fast_compress_tile(const Job& j, std::uint64_t tile, std::uint32_t* s_rmax)
+__device__ __forceinline__ void fast_compress_tile(const Job& j, std::uint64_t tile, std::uint32_t* s_rmax,
+                                                   std::uint32_t* s_stage)
 {
   using Cfg = fast_cfg<T, BITS, NT, RPW_>;
   using U = typename Cfg::U;
@@ -456,15 +471,39 @@ __device__ __forceinline__ void fast_compress_tile(const Job& j, std::uint64_t t
         const std::uint32_t f = (S + 31u) >> 5;
         const int d = (int)(f * 32u - S);
         const int k = (int)(((S + L + 31u) >> 5) - f);
+        if constexpr (FRSZ2_STAGE_UNALIGNED_ROWS) {
+          // the row's L words go through shared memory so they leave as
+          // coalesced 128-bit stores (a row is 4 L bytes, a multiple of 16)
+          std::uint32_t* st = s_stage + warp * L;
 #pragma unroll
-        for (int i = 0; i < NW; ++i) {
-          if (i < k) {
-            const std::uint32_t w = __funnelshift_r(seg[i], seg[i + 1], d);
-            const std::uint32_t off = row_byte + 4u * (f + (std::uint32_t)i);
-            if (full)
-              __stcs(reinterpret_cast<unsigned int*>(dst + off), w);
-            else if (off < wb)
-              store_word_bounded(dst, off, wb, w);
+          for (int i = 0; i < NW; ++i)
+            if (i < k) st[f + i] = __funnelshift_r(seg[i], seg[i + 1], d);
+          __syncwarp();
+          const uint4* st4 = reinterpret_cast<const uint4*>(st);
+          for (int q = lane; q < L / 4; q += 32) {
+            const std::uint32_t off = row_byte + 16u * (std::uint32_t)q;
+            const uint4 v = st4[q];
+            if (full || off + 16u <= wb) {
+              __stcs(reinterpret_cast<uint4*>(dst + off), v);
+            } else if (off < wb) {
+              const std::uint32_t vw[4] = { v.x, v.y, v.z, v.w };
+#pragma unroll
+              for (int t = 0; t < 4; ++t)
+                if (off + 4u * t < wb) store_word_bounded(dst, off + 4u * t, wb, vw[t]);
+            }
+          }
+          __syncwarp(); // the next row reuses the buffer
+        } else {
+#pragma unroll
+          for (int i = 0; i < NW; ++i) {
+            if (i < k) {
+              const std::uint32_t w = __funnelshift_r(seg[i], seg[i + 1], d);
+              const std::uint32_t off = row_byte + 4u * (f + (std::uint32_t)i);
+              if (full)
+                __stcs(reinterpret_cast<unsigned int*>(dst + off), w);
+              else if (off < wb)
+                store_word_bounded(dst, off, wb, w);
+            }
           }
         }
       }
@@ -476,8 +515,9 @@ template<class T, int BITS, int NT = kNT, int RPW = 2>
 __global__ void __launch_bounds__(NT) k_compress_fast(Job j)
 {
   __shared__ std::uint32_t s_rmax[2 * fast_cfg<T, BITS, NT, RPW>::ROWS];
+  __shared__ __align__(16) std::uint32_t s_stage[stage_words<T, BITS, NT, RPW>::value];
   for (std::uint64_t tile = blockIdx.x; tile < j.tiles; tile += gridDim.x)
-    fast_compress_tile<T, BITS, NT, RPW>(j, tile, s_rmax);
+    fast_compress_tile<T, BITS, NT, RPW>(j, tile, s_rmax, s_stage);
 }
 
 // ---------------------------------------------------------------- decompress
