@@ -29,6 +29,15 @@ __global__ void __launch_bounds__(NT)
     while (cur + 1 < nitems && items[cur + 1].tile_begin <= t) ++cur;
     const Job j = items[cur].job;
     const std::uint64_t lt = t - items[cur].tile_begin;
+    if constexpr (!fast_cfg<T, BITS, NT, RPW>::ALIGNED) {
+      if (job_padded(j)) {
+        if (COMPRESS)
+          fast_compress_tile<T, BITS, NT, RPW, true>(j, lt, s_rmax, s_stage);
+        else
+          fast_decompress_tile<T, BITS, NT, RPW, true>(j, lt);
+        continue;
+      }
+    }
     if (COMPRESS)
       fast_compress_tile<T, BITS, NT, RPW>(j, lt, s_rmax, s_stage);
     else

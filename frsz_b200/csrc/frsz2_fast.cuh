@@ -290,23 +290,23 @@ __device__ __forceinline__ typename fp<T>::U decode_plain(typename fast_cfg<T, B
 
 // ---------------------------------------------------------------- compress
 
-#ifndef FRSZ2_STAGE_UNALIGNED_ROWS
-#define FRSZ2_STAGE_UNALIGNED_ROWS 1
-#endif
-
-// Shared-memory words a CTA needs to stage its warps' packed rows (only the
-// unaligned widths stage; one row of L words per warp, 16-byte aligned).
+// Shared-memory words a CTA needs to stage its warps' packed rows: only the
+// unaligned widths stage, one row per warp.  A row holds L words of codes plus,
+// when exponent blocks are padded to whole W-bit words, under W bits of pad per
+// block and at most 32 blocks per row (< 64 words); L + 64 keeps each warp's
+// slice a multiple of 16 bytes.
 template<class T, int BITS, int NT, int RPW>
 struct stage_words
 {
   using Cfg = fast_cfg<T, BITS, NT, RPW>;
-  static constexpr int value = (!Cfg::ALIGNED && FRSZ2_STAGE_UNALIGNED_ROWS) ? Cfg::WARPS * Cfg::L : 4;
+  static constexpr int per_warp = Cfg::ALIGNED ? 0 : Cfg::L + 64;
+  static constexpr int value = Cfg::ALIGNED ? 4 : Cfg::WARPS * per_warp;
 };
 
 // One tile of compress.  s_rmax: 2 * Cfg::ROWS words of shared memory (used
 // only when an exponent block spans several warp rows); s_stage:
 // stage_words<>::value words, 16-byte aligned.
-template<class T, int BITS, int NT, int RPW_>
+template<class T, int BITS, int NT, int RPW_, bool PAD = false>
 __device__ __forceinline__ void fast_compress_tile(const Job& j, std::uint64_t tile, std::uint32_t* s_rmax,
                                                    std::uint32_t* s_stage)
 {
@@ -414,6 +414,12 @@ __device__ __forceinline__ void fast_compress_tile(const Job& j, std::uint64_t t
       __syncthreads();
     }
 
+    // Unpadded blocks: a row is ROW * BITS / 8 bytes.  Padded blocks (E * BITS
+    // not a multiple of W, so E <= 32 < ROW): a row is ROW / E whole blocks.
+    // PAD is the caller's compile-time promise about E * BITS % W.
+    const std::uint32_t blk_bits = 8u * j.block_bytes;
+    const std::uint32_t pad_bits = blk_bits - (std::uint32_t)E * BITS;
+    const std::uint32_t row_bytes = PAD ? (std::uint32_t)(ROW >> log2E) * j.block_bytes : (std::uint32_t)(ROW * BITS / 8);
     const int last_cnt = rem - (nbt - 1) * E;
     const std::uint32_t wb = full ? (std::uint32_t)TB * j.block_bytes
                                   : (std::uint32_t)(nbt - 1) * j.block_bytes + written_block_bytes(last_cnt, BITS, W);
@@ -441,13 +447,13 @@ __device__ __forceinline__ void fast_compress_tile(const Job& j, std::uint64_t t
       if ((idx & (E - 1)) == 0 && bl < nbt)
         store_word(j.exps + (b0 + (std::uint64_t)bl) * (std::uint64_t)(W / 8), (std::uint64_t)be, W);
 
-      std::uint32_t seg[NW + 1];
+      std::uint32_t seg[NW + 3];
 #pragma unroll
-      for (int i = 0; i <= NW; ++i) seg[i] = 0;
+      for (int i = 0; i < NW + 3; ++i) seg[i] = 0;
       pack_all<0, BITS>(seg, c);
 
-      // stream bits of this row start at row * ROW * BITS (a word boundary)
-      const std::uint32_t row_byte = (std::uint32_t)row * (std::uint32_t)(ROW * BITS / 8);
+      // a row's stream bytes are contiguous and start on a 16-byte boundary
+      const std::uint32_t row_byte = (std::uint32_t)row * row_bytes;
       if constexpr (Cfg::ALIGNED) {
         const std::uint32_t off = row_byte + (std::uint32_t)lane * (std::uint32_t)(L / 8);
         std::uint32_t out[NW];
@@ -461,69 +467,76 @@ __device__ __forceinline__ void fast_compress_tile(const Job& j, std::uint64_t t
             if (off + 4u * i < wb) store_word_bounded(dst, off + 4u * i, wb, out[i]);
         }
       } else {
-        // words whose first bit lies in this lane's segment; the tail of the
-        // last one comes from the next lane's first word
+        // The lane writes the stream words whose first bit lies in [S, Sn):
+        // S is its first stream bit, Sn the next lane's (S + L, plus the
+        // block's pad after the last lane of a padded exponent block).  Bits
+        // past the segment are zero pad, then the next lane's first bits,
+        // which one shuffle brings.  The row's words go through shared memory
+        // so they leave as coalesced 16-byte stores.
         const std::uint32_t h0 = __shfl_down_sync(0xFFFFFFFFu, seg[0], 1);
-        constexpr int q = L / 32, r = L % 32;
-        seg[q] |= h0 << r;
-        seg[q + 1] = h0 >> (32 - r);
-        const std::uint32_t S = (std::uint32_t)lane * L;
-        const std::uint32_t f = (S + 31u) >> 5;
-        const int d = (int)(f * 32u - S);
-        const int k = (int)(((S + L + 31u) >> 5) - f);
-        if constexpr (FRSZ2_STAGE_UNALIGNED_ROWS) {
-          // the row's L words go through shared memory so they leave as
-          // coalesced 128-bit stores (a row is 4 L bytes, a multiple of 16)
-          std::uint32_t* st = s_stage + warp * L;
+        std::uint32_t* st = s_stage + warp * stage_words<T, BITS, NT, RPW_>::per_warp;
+        if constexpr (PAD) {
+          const int g = lane & (G - 1);
+          const std::uint32_t S = (std::uint32_t)((lane * P) >> log2E) * blk_bits + (std::uint32_t)g * L;
+          const std::uint32_t Sn = S + L + (g == G - 1 ? pad_bits : 0u);
+          const std::uint32_t f = (S + 31u) >> 5;
+          const int d = (int)(f * 32u - S);
+          const int k = (int)(((Sn + 31u) >> 5) - f);
+          const int sh = (int)(Sn & 31u);
+#pragma unroll
+          for (int i = 0; i < NW + 2; ++i) {
+            if (i < k) {
+              std::uint32_t w = __funnelshift_r(seg[i], seg[i + 1], d);
+              if (i == k - 1 && sh != 0) w |= h0 << sh;
+              st[f + i] = w;
+            }
+          }
+        } else {
+          // unpadded: Sn = S + L at a compile-time offset within the segment
+          constexpr int q = L / 32, r = L % 32;
+          seg[q] |= h0 << r;
+          seg[q + 1] = h0 >> (32 - r);
+          const std::uint32_t S = (std::uint32_t)lane * L;
+          const std::uint32_t f = (S + 31u) >> 5;
+          const int d = (int)(f * 32u - S);
+          const int k = (int)(((S + L + 31u) >> 5) - f);
 #pragma unroll
           for (int i = 0; i < NW; ++i)
             if (i < k) st[f + i] = __funnelshift_r(seg[i], seg[i + 1], d);
-          __syncwarp();
-          const uint4* st4 = reinterpret_cast<const uint4*>(st);
-          for (int q = lane; q < L / 4; q += 32) {
-            const std::uint32_t off = row_byte + 16u * (std::uint32_t)q;
-            const uint4 v = st4[q];
-            if (full || off + 16u <= wb) {
-              __stcs(reinterpret_cast<uint4*>(dst + off), v);
-            } else if (off < wb) {
-              const std::uint32_t vw[4] = { v.x, v.y, v.z, v.w };
+        }
+        __syncwarp();
+        const uint4* st4 = reinterpret_cast<const uint4*>(st);
+        for (int q = lane; q < (PAD ? (int)(row_bytes >> 4) : L / 4); q += 32) {
+          const std::uint32_t off = row_byte + 16u * (std::uint32_t)q;
+          const uint4 v = st4[q];
+          if (full || off + 16u <= wb) {
+            __stcs(reinterpret_cast<uint4*>(dst + off), v);
+          } else if (off < wb) {
+            const std::uint32_t vw[4] = { v.x, v.y, v.z, v.w };
 #pragma unroll
-              for (int t = 0; t < 4; ++t)
-                if (off + 4u * t < wb) store_word_bounded(dst, off + 4u * t, wb, vw[t]);
-            }
-          }
-          __syncwarp(); // the next row reuses the buffer
-        } else {
-#pragma unroll
-          for (int i = 0; i < NW; ++i) {
-            if (i < k) {
-              const std::uint32_t w = __funnelshift_r(seg[i], seg[i + 1], d);
-              const std::uint32_t off = row_byte + 4u * (f + (std::uint32_t)i);
-              if (full)
-                __stcs(reinterpret_cast<unsigned int*>(dst + off), w);
-              else if (off < wb)
-                store_word_bounded(dst, off, wb, w);
-            }
+            for (int t = 0; t < 4; ++t)
+              if (off + 4u * t < wb) store_word_bounded(dst, off + 4u * t, wb, vw[t]);
           }
         }
+        __syncwarp(); // the next row reuses the buffer
       }
     }
   }
 }
 
-template<class T, int BITS, int NT = kNT, int RPW = 2>
+template<class T, int BITS, int NT = kNT, int RPW = 2, bool PAD = false>
 __global__ void __launch_bounds__(NT) k_compress_fast(Job j)
 {
   __shared__ std::uint32_t s_rmax[2 * fast_cfg<T, BITS, NT, RPW>::ROWS];
   __shared__ __align__(16) std::uint32_t s_stage[stage_words<T, BITS, NT, RPW>::value];
   for (std::uint64_t tile = blockIdx.x; tile < j.tiles; tile += gridDim.x)
-    fast_compress_tile<T, BITS, NT, RPW>(j, tile, s_rmax, s_stage);
+    fast_compress_tile<T, BITS, NT, RPW, PAD>(j, tile, s_rmax, s_stage);
 }
 
 // ---------------------------------------------------------------- decompress
 
 // One tile of decompress.
-template<class T, int BITS, int NT, int RPW_>
+template<class T, int BITS, int NT, int RPW_, bool PAD = false>
 __device__ __forceinline__ void fast_decompress_tile(const Job& j, std::uint64_t tile)
 {
   using Cfg = fast_cfg<T, BITS, NT, RPW_>;
@@ -534,8 +547,9 @@ __device__ __forceinline__ void fast_decompress_tile(const Job& j, std::uint64_t
 
   T* __restrict__ y = static_cast<T*>(j.values_out);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int log2E = j.log2E;
+  const int E = j.E, log2E = j.log2E;
   const int TB = (int)j.tile_blocks;
+  const std::uint32_t blk_bits = 8u * j.block_bytes;
 
   {
     const std::uint64_t e0 = tile * (std::uint64_t)TE;
@@ -554,7 +568,10 @@ __device__ __forceinline__ void fast_decompress_tile(const Job& j, std::uint64_t
       const int idx = row * ROW + lane * P;
       if (!full && idx >= rem) continue;
       be[rr] = load_exp(j.exps + (b0 + (std::uint64_t)(idx >> log2E)) * (std::uint64_t)(W / 8), W);
-      const std::uint32_t S = (std::uint32_t)idx * BITS; // tile stream bit
+      // tile stream bit (blocks may end in pad bits when E * BITS is not a
+      // multiple of W; only the unaligned widths take padded blocks)
+      const std::uint32_t S = PAD ? (std::uint32_t)(idx >> log2E) * blk_bits + (std::uint32_t)(idx & (E - 1)) * BITS
+                                  : (std::uint32_t)idx * BITS;
       if constexpr (Cfg::ALIGNED) {
         std::uint32_t t[NW];
         load_words<NW>(src + (S >> 5), t);
@@ -581,7 +598,9 @@ __device__ __forceinline__ void fast_decompress_tile(const Job& j, std::uint64_t
 #pragma unroll
         for (int i = 0; i <= NW; ++i) seg[i] = wv[rr][i];
       } else {
-        const int o = (int)(((std::uint32_t)idx * BITS) & 31u);
+        const int o = (int)((PAD ? (std::uint32_t)(idx >> log2E) * blk_bits + (std::uint32_t)(idx & (E - 1)) * BITS
+                                 : (std::uint32_t)idx * BITS) &
+                            31u);
 #pragma unroll
         for (int i = 0; i < NW; ++i) seg[i] = __funnelshift_r(wv[rr][i], wv[rr][i + 1], o);
         seg[NW] = 0;
@@ -621,11 +640,18 @@ __device__ __forceinline__ void fast_decompress_tile(const Job& j, std::uint64_t
   }
 }
 
-template<class T, int BITS, int NT = kNT, int RPW = 2>
+template<class T, int BITS, int NT = kNT, int RPW = 2, bool PAD = false>
 __global__ void __launch_bounds__(NT) k_decompress_fast(Job j)
 {
   for (std::uint64_t tile = blockIdx.x; tile < j.tiles; tile += gridDim.x)
-    fast_decompress_tile<T, BITS, NT, RPW>(j, tile);
+    fast_decompress_tile<T, BITS, NT, RPW, PAD>(j, tile);
+}
+
+// Whether a job's exponent blocks end in pad bits (E * bits not a multiple of
+// W); the fast kernels take such jobs only for widths with unaligned segments.
+__host__ __device__ inline bool job_padded(const Job& j)
+{
+  return 8ull * j.block_bytes != (std::uint64_t)j.E * (std::uint64_t)j.bits;
 }
 
 // Requirements of the fast kernels for (dtype, bits, E) and pointers, beyond
@@ -636,7 +662,10 @@ __host__ inline bool fast_eligible(const Job& j, int dtype_is_f64, const void* v
   const int TE = dtype_is_f64 ? 2048 : 4096;
   const int E = j.E;
   if (E < P || E > TE || (E & (E - 1)) != 0) return false;
-  if (((std::uint64_t)E * (std::uint64_t)j.bits) % (std::uint64_t)j.W != 0) return false; // no block pad
+  // padded blocks (E * bits not a multiple of W) only for widths whose lane
+  // segments are not word-aligned: those kernels place each lane's bits
+  // by its stream position
+  if (((std::uint64_t)E * (std::uint64_t)j.bits) % (std::uint64_t)j.W != 0 && (P * j.bits) % 32 == 0) return false;
   if (dtype_is_f64 && j.bits < 8) return false;
   if (reinterpret_cast<std::uintptr_t>(values) % 32 != 0) return false;
   if (reinterpret_cast<std::uintptr_t>(words) % 32 != 0) return false;

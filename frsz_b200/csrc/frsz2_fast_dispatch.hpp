@@ -12,6 +12,15 @@ namespace frsz2b {
 template<class T, int BITS>
 cudaError_t launch_fast_one(bool compress, const Job& j, cudaStream_t s, unsigned grid)
 {
+  if constexpr (!fast_cfg<T, BITS>::ALIGNED) {
+    if (job_padded(j)) {
+      if (compress)
+        k_compress_fast<T, BITS, kNT, 2, true><<<grid, kNT, 0, s>>>(j);
+      else
+        k_decompress_fast<T, BITS, kNT, 2, true><<<grid, kNT, 0, s>>>(j);
+      return cudaGetLastError();
+    }
+  }
   if (compress)
     k_compress_fast<T, BITS><<<grid, kNT, 0, s>>>(j);
   else

@@ -104,3 +104,30 @@ def test_batch_rejects_misaligned_pointers(cuda):
     buf = torch.zeros(frsz_b200.compressed_size(np.float64, 32, 32, 100) + 8, dtype=torch.uint8, device="cuda")
     with pytest.raises(frsz_b200.Frsz2Error, match="misaligned"):
         BatchPlan([BatchArray(values=x[1:], compressed=buf[2:], bits=32, block_size=32)])
+
+
+def test_batch_padded_and_unpadded_blocks_in_one_class(cuda):
+    """Arrays of one (float type, width) class whose exponent blocks end in pad
+    bits (E * bits not a multiple of the word width) next to unpadded ones:
+    the persistent kernel picks the padded tile body per array."""
+    specs = [(np.float32, 30_001, 21, 8), (np.float32, 20_000, 21, 32), (np.float32, 4096 * 3, 21, 16),
+             (np.float64, 10_007, 33, 32), (np.float64, 6_000, 33, 64), (np.float64, 2048 * 2 + 9, 33, 4),
+             (np.float64, 9_000, 13, 4), (np.float64, 9_000, 13, 16), (np.float32, 7_000, 13, 8)]
+    arrays, host = make_batch(specs, seed=5)
+    plan = BatchPlan(arrays)
+    info = plan.info()
+    assert info["separate_launches"] == 0 and info["persistent_arrays"] == len(specs)
+    plan.compress()
+    plan.decompress()
+    torch.cuda.synchronize()
+    check_batch(arrays, host)
+    plan.autotune(compress=True)
+    plan.autotune(compress=False)
+    for a in arrays:
+        a.compressed.fill_(0x3D)
+        a.decompressed.fill_(float("nan"))
+    plan.compress()
+    plan.decompress()
+    torch.cuda.synchronize()
+    check_batch(arrays, host)
+    plan.close()
