@@ -14,7 +14,11 @@ TOL = 1e-12
 
 
 @pytest.mark.parametrize("bits,E,n,m", [(32, 32, 100_003, 20), (21, 32, 65_536, 7), (16, 64, 10_001, 33),
-                                        (64, 16, 5_000, 3), (24, 32, 777, 1)])
+                                        (64, 16, 5_000, 3), (24, 32, 777, 1),
+                                        # code stream ending off a 16-byte boundary
+                                        (21, 32, 100_003, 5), (48, 4, 70_001, 4),
+                                        # exponent blocks longer than a slice of the dot
+                                        (16, 4096, 300_001, 3), (32, 65536, 200_000, 2)])
 def test_dot_and_axpy(cuda, bits, E, n, m):
     basis = CompressedBasis(m, n, bits=bits, block_size=E)
     g = torch.Generator(device="cuda").manual_seed(bits + m)
@@ -47,3 +51,18 @@ def test_partial_basis_and_errors(cuda):
     bad.append(torch.ones(100, device="cuda", dtype=torch.float64))
     with pytest.raises(frsz_b200.Frsz2Error, match="no instance for 17 bits"):
         bad.dot(torch.ones(100, device="cuda", dtype=torch.float64))
+
+
+def test_dot_with_w_not_32_byte_aligned(cuda):
+    """w as a view at an 8-byte offset: the dot reads it with scalar loads."""
+    n, m = 50_001, 6
+    basis = CompressedBasis(m, n, bits=32, block_size=32)
+    g = torch.Generator(device="cuda").manual_seed(7)
+    for j in range(m):
+        basis.append(torch.randn(n, generator=g, device="cuda", dtype=torch.float64))
+    V = torch.stack([basis.get(j) for j in range(m)])
+    wbig = torch.randn(n + 1, generator=g, device="cuda", dtype=torch.float64)
+    w = wbig[1:]
+    assert w.data_ptr() % 32 != 0
+    h = basis.dot(w)
+    assert torch.all((h - V @ w).abs() <= TOL * (V.abs() @ w.abs()) + 1e-300)
