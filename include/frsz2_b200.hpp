@@ -12,8 +12,11 @@
 //           GPU happen inside the call
 //       compress_gpu_impl / decompress_gpu_impl  -- DEVICE buffers, stream
 //           ordered, asynchronous
-//       decompress_gpu_elements                  -- random access
-//           (decompress_gpu_element, include/frsz2.hpp:1096-1104)
+//       decompress_gpu_elements                  -- random access from the
+//           host: device indices in, device values out
+//       decompress_gpu_element (device code)     -- random access inside the
+//           caller's own kernels (include/frsz2.hpp:1096-1104); compiled
+//           when the including file is built by nvcc
 //   frsz::int_list_t, frsz::dispatch_frsz2_compression /
 //   dispatch_frsz2_decompression  (include/frsz2.hpp:1292-1347)
 //     same signatures and std::runtime_error messages; host buffers.
@@ -32,6 +35,10 @@
 #include <type_traits>
 
 #include <cuda_runtime_api.h>
+
+#if defined(__CUDACC__)
+#include "frsz2_b200_device.cuh"
+#endif
 
 namespace frsz {
 
@@ -153,6 +160,18 @@ struct frsz2_compressor
     detail::check(frsz2_decompress_elements(detail::dtype_code<fp_type>(), bits_per_value, max_exp_block_size, data_,
                                             total_elements_, d_idx, count, d_output, stream));
   }
+
+#if defined(__CUDACC__)
+  // Value idx, read in device code: pass the view to a kernel by value and
+  // call this per index (the buffer must be device-accessible).  The result
+  // equals decompress_cpu_impl's value idx bit for bit; idx must be below
+  // get_total_elements().
+  __device__ fp_type decompress_gpu_element(std::size_t idx) const
+  {
+    return frsz2_b200::device::decode_element<bits_per_value, max_exp_block_size, fp_type>(exponents_, compressed_,
+                                                                                         idx);
+  }
+#endif
 
 private:
   std::uint8_t* const data_;
