@@ -14,6 +14,7 @@ from .codec import (
     compressed_size,
     decompress,
     decompress_elements,
+    decompress_elements_host,
     decompress_host,
     dispatch_frsz2_compression,
     dispatch_frsz2_decompression,
@@ -28,6 +29,6 @@ from . import serve
 __all__ = [
     "FRSZ2_DOUBLE", "FRSZ2_EDTYPE", "FRSZ2_EFAIL", "FRSZ2_FLOAT", "FRSZ2_OK", "Frsz2Error", "lib",
     "Frsz2Compressor", "compress", "compress_host", "compressed_size", "decompress", "decompress_elements",
-    "decompress_host", "dispatch_frsz2_compression", "dispatch_frsz2_decompression", "exponent_size", "word_bits",
+    "decompress_elements_host", "decompress_host", "dispatch_frsz2_compression", "dispatch_frsz2_decompression", "exponent_size", "word_bits",
     "Frsz2Plugin", "BatchArray", "BatchPlan", "CompressedBasis",
 ]

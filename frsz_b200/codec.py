@@ -155,6 +155,21 @@ def decompress_host(compressed: np.ndarray, n: int, dtype, bits: int, block_size
     return out
 
 
+def decompress_elements_host(compressed: np.ndarray, n: int, dtype, bits: int, block_size: int,
+                             indices: np.ndarray, out: Optional[np.ndarray] = None) -> np.ndarray:
+    """Random-access decode on host buffers (decompress_cpu_element,
+    include/frsz2.hpp:1199-1214): the blocks holding the requested indices
+    are decoded on the GPU.  Indices >= n leave their output untouched."""
+    code = dtype_code(dtype)
+    compressed = np.ascontiguousarray(compressed, dtype=np.uint8)
+    idx = np.ascontiguousarray(indices, dtype=np.uint64)
+    if out is None:
+        out = np.zeros(idx.size, dtype=np.float32 if code == FRSZ2_FLOAT else np.float64)
+    check(lib().frsz2_decompress_elements_host(code, bits, block_size, compressed.ctypes.data, n, idx.ctypes.data,
+                                               idx.size, out.ctypes.data))
+    return out
+
+
 # ------------------------------------------------------------------ class view
 
 class Frsz2Compressor:
@@ -227,6 +242,16 @@ class Frsz2Compressor:
     def decompress_host_impl(self, out: np.ndarray) -> None:
         decompress_host(self.buffer, self.total_elements, self.fp_type, self.bits_per_value,
                         self.max_exp_block_size, out=out)
+
+    def decompress_cpu_element(self, idx: int):
+        """Value idx (include/frsz2.hpp:1199-1214); a host (numpy) buffer goes
+        through the host-buffer call, a CUDA buffer through the device one."""
+        if isinstance(self.buffer, torch.Tensor) and self.buffer.is_cuda:
+            i = torch.tensor([idx], dtype=torch.int64, device=self.buffer.device)
+            return self.decompress_gpu_elements(i).item()
+        return decompress_elements_host(np.asarray(self.buffer), self.total_elements, self.fp_type,
+                                        self.bits_per_value, self.max_exp_block_size,
+                                        np.array([idx], dtype=np.uint64))[0]
 
     def decompress_gpu_elements(self, indices: torch.Tensor) -> torch.Tensor:
         """decompress_gpu_element (include/frsz2.hpp:1096-1104) for a batch

@@ -242,6 +242,18 @@ int ensure(void** p, std::size_t* cap, std::size_t want)
   return FRSZ2_OK;
 }
 
+// Streams and event of a device's staging (first use; caller holds S.mu).
+int staging_init(Staging& S)
+{
+  if (S.init) return FRSZ2_OK;
+  int rc;
+  for (auto& s : S.st)
+    if ((rc = cuda_status(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "stream create"))) return rc;
+  if ((rc = cuda_status(cudaEventCreateWithFlags(&S.ev_start, cudaEventDisableTiming), "event create"))) return rc;
+  S.init = true;
+  return FRSZ2_OK;
+}
+
 // Slices of whole tiles so every slice keeps the tile kernel's alignment.
 std::uint64_t slice_blocks(const Layout& L, int dtype)
 {
@@ -268,12 +280,7 @@ int host_codec(bool compress, int dtype, int bits, int E, const void* h_in, std:
   if (dev < 0 || dev >= 64) return set_error(FRSZ2_EFAIL, "device index out of range");
   Staging& S = g_staging[dev];
   std::lock_guard<std::mutex> lock(S.mu);
-  if (!S.init) {
-    for (auto& s : S.st)
-      if ((rc = cuda_status(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "stream create"))) return rc;
-    if ((rc = cuda_status(cudaEventCreateWithFlags(&S.ev_start, cudaEventDisableTiming), "event create"))) return rc;
-    S.init = true;
-  }
+  if ((rc = staging_init(S))) return rc;
   const std::size_t es = dtype == FRSZ2_FLOAT ? 4 : 8;
   if ((rc = ensure(&S.d_values, &S.values_cap, L.n * es))) return rc;
   if ((rc = ensure(&S.d_buf, &S.buf_cap, L.total_bytes))) return rc;
@@ -470,6 +477,76 @@ int frsz2_decompress_elements(int dtype, int bits, int block_size, const void* d
   else
     k_decompress_elements<double><<<grid, kNT, 0, s>>>(j, d_idx, count, static_cast<double*>(d_out));
   return cuda_status(cudaGetLastError(), "element decode launch");
+}
+
+// Host-buffer random access (decompress_cpu_element, include/frsz2.hpp:1199-1214):
+// the host gathers the exponent and block bytes of every block a valid index
+// falls in into a small buffer laid out as an array of those blocks, which
+// the element kernel decodes on the GPU.
+int frsz2_decompress_elements_host(int dtype, int bits, int block_size, const void* h_compressed, uint64_t n,
+                                   const uint64_t* h_idx, uint64_t count, void* h_out)
+{
+  NvtxRange nvtx("frsz2_decompress_elements_host");
+  int rc = check_args(dtype, bits, block_size);
+  if (rc) return rc;
+  if (count == 0) return FRSZ2_OK;
+  if (!h_compressed || !h_idx || !h_out) return set_error(FRSZ2_EFAIL, "null pointer");
+  const Layout L = make_layout(n, bits, block_size);
+  const std::uint64_t E = (std::uint64_t)block_size, EB = (std::uint64_t)(L.W / 8), BB = L.block_bytes;
+  std::vector<std::uint64_t> blocks;
+  blocks.reserve(count);
+  for (std::uint64_t t = 0; t < count; ++t)
+    if (h_idx[t] < n) blocks.push_back(h_idx[t] / E);
+  if (blocks.empty()) return FRSZ2_OK; // every index out of range: outputs untouched
+  std::sort(blocks.begin(), blocks.end());
+  blocks.erase(std::unique(blocks.begin(), blocks.end()), blocks.end());
+  const std::uint64_t m = blocks.size();
+  const Layout M = make_layout(m * E, bits, block_size);
+  const std::uint8_t* hb = static_cast<const std::uint8_t*>(h_compressed);
+  std::vector<std::uint8_t> mini(M.total_bytes, 0);
+  for (std::uint64_t k = 0; k < m; ++k) {
+    std::memcpy(mini.data() + k * EB, hb + blocks[k] * EB, EB);
+    std::memcpy(mini.data() + M.exp_bytes + k * BB, hb + L.exp_bytes + blocks[k] * BB, BB);
+  }
+  std::vector<std::uint64_t> mapped(count);
+  for (std::uint64_t t = 0; t < count; ++t) {
+    const std::uint64_t g = h_idx[t];
+    if (g >= n) {
+      mapped[t] = ~0ull; // the kernel skips it
+      continue;
+    }
+    const std::uint64_t k = (std::uint64_t)(std::lower_bound(blocks.begin(), blocks.end(), g / E) - blocks.begin());
+    mapped[t] = k * E + g % E;
+  }
+
+  int dev = 0;
+  if ((rc = cuda_status(cudaGetDevice(&dev), "cudaGetDevice"))) return rc;
+  if (dev < 0 || dev >= 64) return set_error(FRSZ2_EFAIL, "device index out of range");
+  Staging& S = g_staging[dev];
+  std::lock_guard<std::mutex> lock(S.mu);
+  if ((rc = staging_init(S))) return rc;
+  const std::size_t es = dtype == FRSZ2_FLOAT ? 4 : 8;
+  const std::size_t idx_off = (M.total_bytes + 255) / 256 * 256;
+  if ((rc = ensure(&S.d_buf, &S.buf_cap, idx_off + count * sizeof(std::uint64_t)))) return rc;
+  if ((rc = ensure(&S.d_values, &S.values_cap, count * es))) return rc;
+  std::uint8_t* d_buf = static_cast<std::uint8_t*>(S.d_buf);
+  auto* d_idx = reinterpret_cast<std::uint64_t*>(d_buf + idx_off);
+  cudaStream_t s = S.st[0];
+  if ((rc = cuda_status(cudaMemcpyAsync(d_buf, mini.data(), M.total_bytes, cudaMemcpyHostToDevice, s), "H2D")) ||
+      (rc = cuda_status(cudaMemcpyAsync(d_idx, mapped.data(), count * sizeof(std::uint64_t), cudaMemcpyHostToDevice,
+                                        s),
+                        "H2D")) ||
+      (rc = cuda_status(cudaMemcpyAsync(S.d_values, h_out, count * es, cudaMemcpyHostToDevice, s), "H2D")))
+    return rc;
+  Job j = job_for_slice(M, dtype, 0, M.nb, nullptr, nullptr, d_buf);
+  const unsigned grid = grid_for(count, kNT);
+  if (dtype == FRSZ2_FLOAT)
+    k_decompress_elements<float><<<grid, kNT, 0, s>>>(j, d_idx, count, static_cast<float*>(S.d_values));
+  else
+    k_decompress_elements<double><<<grid, kNT, 0, s>>>(j, d_idx, count, static_cast<double*>(S.d_values));
+  if ((rc = cuda_status(cudaGetLastError(), "element decode launch"))) return rc;
+  if ((rc = cuda_status(cudaMemcpyAsync(h_out, S.d_values, count * es, cudaMemcpyDeviceToHost, s), "D2H"))) return rc;
+  return cuda_status(cudaStreamSynchronize(s), "stream synchronize");
 }
 
 } // extern "C"

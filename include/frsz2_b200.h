@@ -98,12 +98,22 @@ int frsz2_decompress_blocks(int dtype, int bits, int block_size, const void* d_c
                             uint64_t block_begin, uint64_t block_count, void* d_values, void* stream);
 
 /* Random-access decode of `count` elements at device indices d_idx[0..count)
- * into d_out.  Replaces decompress_gpu_element (include/frsz2.hpp:1096-1104)
- * and decompress_cpu_element (include/frsz2.hpp:1199-1214); values are
- * bit-exact with the CPU decode (decompress_cpu_element), including the zero
- * code rule, which the reference GPU element decode does not follow. */
+ * into d_out (device buffers), for host code.  The device-side accessor
+ * decompress_gpu_element (include/frsz2.hpp:1096-1104) for use inside kernels
+ * is include/frsz2_b200_device.cuh.  Values are bit-exact with the CPU decode
+ * (decompress_cpu_element), including the zero code rule, which the reference
+ * GPU element decode does not follow.  Indices >= n leave their output
+ * untouched. */
 int frsz2_decompress_elements(int dtype, int bits, int block_size, const void* d_compressed, uint64_t n,
                               const uint64_t* d_idx, uint64_t count, void* d_out, void* stream);
+
+/* The same on HOST buffers: the compressed array, the indices and the outputs
+ * in host memory (decompress_cpu_element, include/frsz2.hpp:1199-1214).  Only
+ * the blocks that hold a requested index are copied to the GPU, decoded there
+ * and the values copied back; the call returns when h_out is written.
+ * Indices >= n leave their output untouched. */
+int frsz2_decompress_elements_host(int dtype, int bits, int block_size, const void* h_compressed, uint64_t n,
+                                   const uint64_t* h_idx, uint64_t count, void* h_out);
 
 /* ---------------------------------------------------------------------------
  * Batched path: no counterpart in the reference (which compresses one array

@@ -142,6 +142,23 @@ struct frsz2_compressor
     return 0;
   }
 
+  // Value idx of a HOST buffer (include/frsz2.hpp:1199-1214): the block that
+  // holds it is decoded on the GPU.
+  fp_type decompress_cpu_element(const std::size_t idx) const
+  {
+    const std::uint64_t i = idx;
+    fp_type v{};
+    detail::check(frsz2_decompress_elements_host(detail::dtype_code<fp_type>(), bits_per_value, max_exp_block_size,
+                                                 data_, total_elements_, &i, 1, &v));
+    return v;
+  }
+  // Values at host indices idx[0..count) of a HOST buffer, in one call.
+  void decompress_cpu_elements(const std::uint64_t* idx, std::size_t count, fp_type* output) const
+  {
+    detail::check(frsz2_decompress_elements_host(detail::dtype_code<fp_type>(), bits_per_value, max_exp_block_size,
+                                                 data_, total_elements_, idx, count, output));
+  }
+
   // Device buffers (the view's buffer and `data` in GPU memory).
   void compress_gpu_impl(const fp_type* d_data, cudaStream_t stream = nullptr)
   {

@@ -80,6 +80,11 @@ static void e2e_case(std::FILE* out, std::size_t n)
   std::vector<T> v(idx.size());
   cudaMemcpy(v.data(), dv, idx.size() * sizeof(T), cudaMemcpyDeviceToHost);
   for (std::size_t i = 0; i < idx.size(); ++i) CHECK(v[i] == x[idx[i]]);
+  // random access on the host buffer, one value and a batch
+  for (std::size_t i = 0; i < idx.size(); ++i) CHECK(host.decompress_cpu_element(idx[i]) == x[idx[i]]);
+  std::vector<T> hv(idx.size());
+  host.decompress_cpu_elements(idx.data(), idx.size(), hv.data());
+  for (std::size_t i = 0; i < idx.size(); ++i) CHECK(hv[i] == x[idx[i]]);
   cudaFree(dx);
   cudaFree(dy);
   cudaFree(db);

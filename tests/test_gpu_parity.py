@@ -213,3 +213,26 @@ def test_compressor_view_and_dispatch(cuda):
     view = frsz_b200.Frsz2Compressor(16, 64, np.float64, buf, n)
     assert torch.equal(view.get_exponent_data().cpu(),
                        torch.from_numpy(ref[: view.get_exponent_data().numel() * 2].view(np.int16).copy()))
+
+
+@pytest.mark.parametrize("dtype,bits,E", [(np.float32, 16, 32), (np.float32, 9, 5), (np.float32, 21, 8),
+                                          (np.float64, 21, 32), (np.float64, 33, 32), (np.float64, 7, 1),
+                                          (np.float64, 64, 1000)])
+def test_host_random_access_matches_oracle(cuda, dtype, bits, E):
+    """frsz2_decompress_elements_host: host buffer, host indices (duplicates,
+    any order, some out of range), host outputs."""
+    rng = np.random.default_rng(bits * 7 + E)
+    n = 10_007
+    lo, hi = (-30, 30) if dtype == np.float64 and bits <= 8 else (-20, 20)
+    x = workloads.loguniform_np(n, dtype, seed=bits + E, lo=lo, hi=hi)
+    x[rng.choice(n, 50, replace=False)] = 0.0
+    x[rng.choice(n, 20, replace=False)] = np.nan
+    ref = oracle.compress(x, bits, E)
+    want = oracle.decompress(ref, n, dtype, bits, E)
+    idx = np.concatenate([rng.integers(0, n, 3000), [0, n - 1, n - 1, 5, n, n + 77, 2 ** 63]]).astype(np.uint64)
+    out = np.full(idx.size, 42.0, dtype=dtype)
+    frsz_b200.decompress_elements_host(ref, n, dtype, bits, E, idx, out=out)
+    valid = idx < n
+    uint = np.uint64 if dtype == np.float64 else np.uint32
+    assert np.array_equal(out[valid].view(uint), want[idx[valid].astype(np.int64)].view(uint))
+    assert np.all(out[~valid] == 42.0)
