@@ -15,9 +15,9 @@ constexpr auto f64_shape0(std::integer_sequence<int, I...>)
 
 batch_entry batch_class_f64(int bits, int shape)
 {
-  static constexpr auto s0 = f64_shape0<8>(std::make_integer_sequence<int, 57>{});
-  if (bits < 8 || bits > 64) return { nullptr, nullptr };
-  if (shape == 0) return s0[bits - 8];
+  static constexpr auto s0 = f64_shape0<4>(std::make_integer_sequence<int, 61>{});
+  if (bits < 4 || bits > 64) return { nullptr, nullptr };
+  if (shape == 0) return s0[bits - 4];
   switch (bits * 4 + shape) {
 #define TUNED(B)                                                                                                   \
   case B * 4 + 1: return { &launch_batch_class<double, B, 128, 2>, &batch_class_occupancy<double, B, 128, 2> };      \

@@ -121,9 +121,14 @@ template<class T>
 static cudaError_t try_fast(bool compress, const Job& j, cudaStream_t s)
 {
   const void* values = compress ? j.values_in : j.values_out;
-  if (!fast_eligible(j, sizeof(T) == 8, values, j.words)) return cudaErrorNotSupported;
   const unsigned grid = (unsigned)std::min<std::uint64_t>(j.tiles, 1u << 30);
-  return sizeof(T) == 8 ? launch_fast_f64(j.bits, compress, j, s, grid) : launch_fast_f32(j.bits, compress, j, s, grid);
+  if (fast_eligible(j, sizeof(T) == 8, values, j.words))
+    return sizeof(T) == 8 ? launch_fast_f64(j.bits, compress, j, s, grid)
+                          : launch_fast_f32(j.bits, compress, j, s, grid);
+  if (small_block_eligible(j, sizeof(T) == 8, values, j.words))
+    return sizeof(T) == 8 ? launch_fast_small_f64(j.bits, j.E, compress, j, s, grid)
+                          : launch_fast_small_f32(j.bits, j.E, compress, j, s, grid);
+  return cudaErrorNotSupported;
 }
 
 template<class T>

@@ -30,13 +30,22 @@
 
 namespace frsz2b {
 
-template<class T, int BITS, int NT_ = kNT, int RPW_ = 2>
+// ESM = 0: exponent blocks of E >= P values (E a runtime power of two).
+// ESM = 1, 2 or 4 (< P): blocks of exactly ESM values, so a lane holds P / ESM
+// whole blocks, each padded to whole W-bit words; value i of a lane then sits
+// at bit (i / ESM) * BBB + (i % ESM) * BITS of its segment.
+template<class T, int BITS, int NT_ = kNT, int RPW_ = 2, int ESM_ = 0>
 struct fast_cfg
 {
   using U = typename fp<T>::U;
   using C = std::conditional_t<(BITS <= 32), std::uint32_t, std::uint64_t>;
+  static constexpr int W = BITS <= 8 ? 8 : BITS <= 16 ? 16 : BITS <= 32 ? 32 : 64;
+  static constexpr int B = BITS;                 // bits per value
   static constexpr int P = 32 / (int)sizeof(T);  // values per lane
-  static constexpr int L = P * BITS;             // segment bits per lane
+  static constexpr int ESM = ESM_;
+  static_assert(ESM == 0 || (ESM < P && (ESM & (ESM - 1)) == 0), "blocks smaller than a lane's values");
+  static constexpr int BBB = ESM ? ((ESM * BITS + W - 1) / W) * W : 0; // bits of one small block
+  static constexpr int L = ESM ? (P / ESM) * BBB : P * BITS;         // segment bits per lane
   static constexpr int NW = (L + 31) / 32;       // segment words
   static constexpr bool ALIGNED = (L % 32) == 0; // segments start on word boundaries
   static constexpr int ROW = 32 * P;             // values per warp row
@@ -45,7 +54,8 @@ struct fast_cfg
   static constexpr int WARPS = NT / 32;
   static constexpr int ROWS = WARPS * RPW;       // rows per tile
   static constexpr int TE = ROWS * ROW;          // values per tile
-  static constexpr int W = BITS <= 8 ? 8 : BITS <= 16 ? 16 : BITS <= 32 ? 32 : 64;
+  // bit of a lane's segment where its value i starts
+  __host__ __device__ static constexpr int pos(int i) { return ESM ? (i / ESM) * BBB + (i % ESM) * BITS : i * BITS; }
 };
 
 // Values per tile of the fast kernels for a CTA width and rows per warp.
@@ -194,6 +204,25 @@ __device__ __forceinline__ void unpack_all(const std::uint32_t (&seg)[N], C (&c)
   }
 }
 
+// pack_all / unpack_all at the positions of a lane configuration (Cfg::pos).
+template<class Cfg, int K = 0, int N, class C, int P>
+__device__ __forceinline__ void pack_lane(std::uint32_t (&seg)[N], const C (&c)[P])
+{
+  if constexpr (K < P) {
+    put_bits<Cfg::pos(K), Cfg::B>(seg, c[K]);
+    pack_lane<Cfg, K + 1>(seg, c);
+  }
+}
+
+template<class Cfg, int K = 0, int N, class C, int P>
+__device__ __forceinline__ void unpack_lane(const std::uint32_t (&seg)[N], C (&c)[P])
+{
+  if constexpr (K < P) {
+    c[K] = (C)get_bits<Cfg::pos(K), Cfg::B>(seg);
+    unpack_lane<Cfg, K + 1>(seg, c);
+  }
+}
+
 // ---------------------------------------------------------------- keys
 
 // Block-max key of a value: the magnitude bits that decide the exponent
@@ -295,22 +324,88 @@ __device__ __forceinline__ typename fp<T>::U decode_plain(typename fast_cfg<T, B
 // when exponent blocks are padded to whole W-bit words, under W bits of pad per
 // block and at most 32 blocks per row (< 64 words); L + 64 keeps each warp's
 // slice a multiple of 16 bytes.
-template<class T, int BITS, int NT, int RPW>
+template<class T, int BITS, int NT, int RPW, int ESM = 0>
 struct stage_words
 {
-  using Cfg = fast_cfg<T, BITS, NT, RPW>;
+  using Cfg = fast_cfg<T, BITS, NT, RPW, ESM>;
   static constexpr int per_warp = Cfg::ALIGNED ? 0 : Cfg::L + 64;
   static constexpr int value = Cfg::ALIGNED ? 4 : Cfg::WARPS * per_warp;
 };
 
+// Store / load the NBL consecutive W-bit exponents of one lane (blocks of
+// fewer values than a lane holds).  p is aligned to their total size (at
+// most 32 bytes); `present` (store) is how many of them exist.
+template<int W, int NBL>
+__device__ __forceinline__ void store_lane_exps(std::uint8_t* p, const std::int64_t (&e)[NBL], int present)
+{
+  constexpr int TBY = NBL * W / 8;
+  if (present >= NBL) {
+    if constexpr (TBY >= 4) {
+      constexpr int NWD = TBY / 4;
+      std::uint32_t wd[NWD];
+#pragma unroll
+      for (int k = 0; k < NWD; ++k) wd[k] = 0;
+#pragma unroll
+      for (int b = 0; b < NBL; ++b) {
+        if constexpr (W == 64) {
+          wd[2 * b] = (std::uint32_t)(std::uint64_t)e[b];
+          wd[2 * b + 1] = (std::uint32_t)((std::uint64_t)e[b] >> 32);
+        } else {
+          constexpr std::uint32_t M = W == 32 ? 0xFFFFFFFFu : ((1u << W) - 1u);
+          wd[(b * W) / 32] |= ((std::uint32_t)e[b] & M) << ((b * W) % 32);
+        }
+      }
+      store_words<NWD>(reinterpret_cast<std::uint32_t*>(p), wd);
+    } else if constexpr (TBY == 2) {
+      *reinterpret_cast<std::uint16_t*>(p) = (std::uint16_t)(((std::uint32_t)e[0] & 0xFFu) | ((std::uint32_t)e[1] & 0xFFu) << 8);
+    } else {
+      *p = (std::uint8_t)e[0];
+    }
+  } else {
+#pragma unroll
+    for (int b = 0; b < NBL; ++b)
+      if (b < present) store_word(p + b * (W / 8), (std::uint64_t)e[b], W);
+  }
+}
+
+// All NBL exponents are read (the bytes past the last block belong to the
+// buffer: the exponent section's pad or the first code words).
+template<int W, int NBL>
+__device__ __forceinline__ void load_lane_exps(const std::uint8_t* p, std::int64_t (&e)[NBL])
+{
+  constexpr int TBY = NBL * W / 8;
+  if constexpr (TBY >= 4) {
+    constexpr int NWD = TBY / 4;
+    std::uint32_t wd[NWD];
+    load_words<NWD>(reinterpret_cast<const std::uint32_t*>(p), wd);
+#pragma unroll
+    for (int b = 0; b < NBL; ++b) {
+      if constexpr (W == 64)
+        e[b] = (std::int64_t)(((std::uint64_t)wd[2 * b + 1] << 32) | wd[2 * b]);
+      else if constexpr (W == 32)
+        e[b] = (std::int32_t)wd[b];
+      else if constexpr (W == 16)
+        e[b] = (std::int16_t)(wd[(b * 16) / 32] >> ((b * 16) % 32));
+      else
+        e[b] = (std::int8_t)(wd[(b * 8) / 32] >> ((b * 8) % 32));
+    }
+  } else if constexpr (TBY == 2) {
+    const std::uint16_t v = __ldg(reinterpret_cast<const unsigned short*>(p));
+    e[0] = (std::int8_t)(v & 0xFFu);
+    e[1] = (std::int8_t)(v >> 8);
+  } else {
+    e[0] = (std::int8_t)__ldg(p);
+  }
+}
+
 // One tile of compress.  s_rmax: 2 * Cfg::ROWS words of shared memory (used
 // only when an exponent block spans several warp rows); s_stage:
 // stage_words<>::value words, 16-byte aligned.
-template<class T, int BITS, int NT, int RPW_, bool PAD = false>
+template<class T, int BITS, int NT, int RPW_, bool PAD = false, int ESM = 0>
 __device__ __forceinline__ void fast_compress_tile(const Job& j, std::uint64_t tile, std::uint32_t* s_rmax,
                                                    std::uint32_t* s_stage)
 {
-  using Cfg = fast_cfg<T, BITS, NT, RPW_>;
+  using Cfg = fast_cfg<T, BITS, NT, RPW_, ESM>;
   using U = typename Cfg::U;
   using C = typename Cfg::C;
   using K = key_of<T>;
@@ -352,7 +447,9 @@ __device__ __forceinline__ void fast_compress_tile(const Job& j, std::uint64_t t
     }
 
     // block maxima: raw keys detect Inf/NaN, clean keys skip NaN like std::max
+    // (blocks within a lane, ESM > 0: computed per block below)
     std::uint32_t km[RPW], kc[RPW];
+    if constexpr (ESM == 0) {
     bool any_special = false;
 #pragma unroll
     for (int rr = 0; rr < RPW; ++rr) {
@@ -413,13 +510,14 @@ __device__ __forceinline__ void fast_compress_tile(const Job& j, std::uint64_t t
       }
       __syncthreads();
     }
+    }
 
     // Unpadded blocks: a row is ROW * BITS / 8 bytes.  Padded blocks (E * BITS
     // not a multiple of W, so E <= 32 < ROW): a row is ROW / E whole blocks.
     // PAD is the caller's compile-time promise about E * BITS % W.
     const std::uint32_t blk_bits = 8u * j.block_bytes;
     const std::uint32_t pad_bits = blk_bits - (std::uint32_t)E * BITS;
-    const std::uint32_t row_bytes = PAD ? (std::uint32_t)(ROW >> log2E) * j.block_bytes : (std::uint32_t)(ROW * BITS / 8);
+    const std::uint32_t row_bytes = PAD ? (std::uint32_t)(ROW >> log2E) * j.block_bytes : (std::uint32_t)(4 * L);
     const int last_cnt = rem - (nbt - 1) * E;
     const std::uint32_t wb = full ? (std::uint32_t)TB * j.block_bytes
                                   : (std::uint32_t)(nbt - 1) * j.block_bytes + written_block_bytes(last_cnt, BITS, W);
@@ -430,27 +528,59 @@ __device__ __forceinline__ void fast_compress_tile(const Job& j, std::uint64_t t
       const int row = rr * Cfg::WARPS + warp;
       const int idx = row * ROW + lane * P;
       const int bl = idx >> log2E;
-      const int field = (int)(kc[rr] >> K::FSHIFT);
-      const std::int64_t ex = exponent_of_field<T>(field);
-      const std::int64_t be = wrap_signed(ex, W);
-      const bool plain = km[rr] < K::SPECIAL && be == ex && plain_exponent<T>(be);
-
       C c[P];
-      if (plain) {
-        const T scale = pow2<T>(BITS - 2 - (int)be);
+      if constexpr (ESM == 0) {
+        const int field = (int)(kc[rr] >> K::FSHIFT);
+        const std::int64_t ex = exponent_of_field<T>(field);
+        const std::int64_t be = wrap_signed(ex, W);
+        const bool plain = km[rr] < K::SPECIAL && be == ex && plain_exponent<T>(be);
+        if (plain) {
+          const T scale = pow2<T>(BITS - 2 - (int)be);
 #pragma unroll
-        for (int i = 0; i < P; ++i) c[i] = encode_plain<T, BITS>(u[rr][i], scale);
+          for (int i = 0; i < P; ++i) c[i] = encode_plain<T, BITS>(u[rr][i], scale);
+        } else {
+#pragma unroll
+          for (int i = 0; i < P; ++i) c[i] = (C)to_code<T>(u[rr][i], (std::int16_t)be, BITS);
+        }
+        if ((idx & (E - 1)) == 0 && bl < nbt)
+          store_word(j.exps + (b0 + (std::uint64_t)bl) * (std::uint64_t)(W / 8), (std::uint64_t)be, W);
       } else {
+        // the lane's P / ESM blocks, each with its own exponent
+        constexpr int NBL = P / ESM;
+        std::int64_t exb[NBL];
 #pragma unroll
-        for (int i = 0; i < P; ++i) c[i] = (C)to_code<T>(u[rr][i], (std::int16_t)be, BITS);
+        for (int b = 0; b < NBL; ++b) {
+          std::uint32_t mr = K::raw(u[rr][b * ESM]);
+#pragma unroll
+          for (int i = 1; i < ESM; ++i) mr = max(mr, K::raw(u[rr][b * ESM + i]));
+          std::uint32_t mc = mr;
+          if (mr >= K::SPECIAL) {
+            mc = K::clean(u[rr][b * ESM]);
+#pragma unroll
+            for (int i = 1; i < ESM; ++i) mc = max(mc, K::clean(u[rr][b * ESM + i]));
+          }
+          const std::int64_t ex = exponent_of_field<T>((int)(mc >> K::FSHIFT));
+          const std::int64_t be = wrap_signed(ex, W);
+          const bool plain = mr < K::SPECIAL && be == ex && plain_exponent<T>(be);
+          if (plain) {
+            const T scale = pow2<T>(BITS - 2 - (int)be);
+#pragma unroll
+            for (int i = 0; i < ESM; ++i) c[b * ESM + i] = encode_plain<T, BITS>(u[rr][b * ESM + i], scale);
+          } else {
+#pragma unroll
+            for (int i = 0; i < ESM; ++i) c[b * ESM + i] = (C)to_code<T>(u[rr][b * ESM + i], (std::int16_t)be, BITS);
+          }
+          exb[b] = be;
+        }
+        const int present = nbt - bl; // blocks of this lane inside the array
+        if (present > 0)
+          store_lane_exps<W, NBL>(j.exps + (b0 + (std::uint64_t)bl) * (std::uint64_t)(W / 8), exb, present);
       }
-      if ((idx & (E - 1)) == 0 && bl < nbt)
-        store_word(j.exps + (b0 + (std::uint64_t)bl) * (std::uint64_t)(W / 8), (std::uint64_t)be, W);
 
       std::uint32_t seg[NW + 3];
 #pragma unroll
       for (int i = 0; i < NW + 3; ++i) seg[i] = 0;
-      pack_all<0, BITS>(seg, c);
+      pack_lane<Cfg>(seg, c);
 
       // a row's stream bytes are contiguous and start on a 16-byte boundary
       const std::uint32_t row_byte = (std::uint32_t)row * row_bytes;
@@ -474,8 +604,24 @@ __device__ __forceinline__ void fast_compress_tile(const Job& j, std::uint64_t t
         // which one shuffle brings.  The row's words go through shared memory
         // so they leave as coalesced 16-byte stores.
         const std::uint32_t h0 = __shfl_down_sync(0xFFFFFFFFu, seg[0], 1);
-        std::uint32_t* st = s_stage + warp * stage_words<T, BITS, NT, RPW_>::per_warp;
-        if constexpr (PAD) {
+        std::uint32_t* st = s_stage + warp * stage_words<T, BITS, NT, RPW_, ESM>::per_warp;
+        if constexpr (L < 32) {
+          // segments shorter than a word (fp64 below 8 bits): up to three
+          // lanes share a word, so each lane ORs its bits into the zeroed
+          // row; pad bits stay zero
+          const int nrw = PAD ? (int)(row_bytes >> 2) : L;
+          for (int q = lane; q < nrw; q += 32) st[q] = 0u;
+          __syncwarp();
+          std::uint32_t S;
+          if constexpr (PAD)
+            S = (std::uint32_t)((lane * P) >> log2E) * blk_bits + (std::uint32_t)(lane & (G - 1)) * L;
+          else
+            S = (std::uint32_t)lane * L;
+          const std::uint32_t w = S >> 5;
+          const int o = (int)(S & 31u);
+          atomicOr(&st[w], seg[0] << o);
+          if (o + L > 32) atomicOr(&st[w + 1], seg[0] >> (32 - o));
+        } else if constexpr (PAD) {
           const int g = lane & (G - 1);
           const std::uint32_t S = (std::uint32_t)((lane * P) >> log2E) * blk_bits + (std::uint32_t)g * L;
           const std::uint32_t Sn = S + L + (g == G - 1 ? pad_bits : 0u);
@@ -524,22 +670,23 @@ __device__ __forceinline__ void fast_compress_tile(const Job& j, std::uint64_t t
   }
 }
 
-template<class T, int BITS, int NT = kNT, int RPW = 2, bool PAD = false>
+template<class T, int BITS, int NT = kNT, int RPW = 2, bool PAD = false, int ESM = 0>
 __global__ void __launch_bounds__(NT) k_compress_fast(Job j)
 {
   __shared__ std::uint32_t s_rmax[2 * fast_cfg<T, BITS, NT, RPW>::ROWS];
-  __shared__ __align__(16) std::uint32_t s_stage[stage_words<T, BITS, NT, RPW>::value];
+  __shared__ __align__(16) std::uint32_t s_stage[stage_words<T, BITS, NT, RPW, ESM>::value];
   for (std::uint64_t tile = blockIdx.x; tile < j.tiles; tile += gridDim.x)
-    fast_compress_tile<T, BITS, NT, RPW, PAD>(j, tile, s_rmax, s_stage);
+    fast_compress_tile<T, BITS, NT, RPW, PAD, ESM>(j, tile, s_rmax, s_stage);
 }
 
 // ---------------------------------------------------------------- decompress
 
 // One tile of decompress.
-template<class T, int BITS, int NT, int RPW_, bool PAD = false>
+template<class T, int BITS, int NT, int RPW_, bool PAD = false, int ESM = 0>
 __device__ __forceinline__ void fast_decompress_tile(const Job& j, std::uint64_t tile)
 {
-  using Cfg = fast_cfg<T, BITS, NT, RPW_>;
+  using Cfg = fast_cfg<T, BITS, NT, RPW_, ESM>;
+  constexpr int NBL = ESM ? Cfg::P / ESM : 1; // exponents per lane
   using U = typename Cfg::U;
   using C = typename Cfg::C;
   constexpr int P = Cfg::P, L = Cfg::L, NW = Cfg::NW, ROW = Cfg::ROW, RPW = Cfg::RPW, TE = Cfg::TE,
@@ -561,17 +708,23 @@ __device__ __forceinline__ void fast_decompress_tile(const Job& j, std::uint64_t
       reinterpret_cast<const std::uint32_t*>(j.words + b0 * (std::uint64_t)j.block_bytes);
 
     std::uint32_t wv[RPW][NW + 1];
-    std::int64_t be[RPW];
+    std::int64_t be[RPW][NBL];
 #pragma unroll
     for (int rr = 0; rr < RPW; ++rr) {
       const int row = rr * Cfg::WARPS + warp;
       const int idx = row * ROW + lane * P;
       if (!full && idx >= rem) continue;
-      be[rr] = load_exp(j.exps + (b0 + (std::uint64_t)(idx >> log2E)) * (std::uint64_t)(W / 8), W);
+      const std::uint8_t* ep = j.exps + (b0 + (std::uint64_t)(idx >> log2E)) * (std::uint64_t)(W / 8);
+      if constexpr (ESM == 0)
+        be[rr][0] = load_exp(ep, W);
+      else
+        load_lane_exps<W, NBL>(ep, be[rr]);
       // tile stream bit (blocks may end in pad bits when E * BITS is not a
-      // multiple of W; only the unaligned widths take padded blocks)
-      const std::uint32_t S = PAD ? (std::uint32_t)(idx >> log2E) * blk_bits + (std::uint32_t)(idx & (E - 1)) * BITS
-                                  : (std::uint32_t)idx * BITS;
+      // multiple of W; only the unaligned widths take padded blocks; blocks
+      // smaller than a lane are padded at compile-time positions)
+      const std::uint32_t S = ESM ? (std::uint32_t)(idx / (ESM ? ESM : 1)) * Cfg::BBB
+                              : PAD ? (std::uint32_t)(idx >> log2E) * blk_bits + (std::uint32_t)(idx & (E - 1)) * BITS
+                                    : (std::uint32_t)idx * BITS;
       if constexpr (Cfg::ALIGNED) {
         std::uint32_t t[NW];
         load_words<NW>(src + (S >> 5), t);
@@ -598,27 +751,32 @@ __device__ __forceinline__ void fast_decompress_tile(const Job& j, std::uint64_t
 #pragma unroll
         for (int i = 0; i <= NW; ++i) seg[i] = wv[rr][i];
       } else {
-        const int o = (int)((PAD ? (std::uint32_t)(idx >> log2E) * blk_bits + (std::uint32_t)(idx & (E - 1)) * BITS
-                                 : (std::uint32_t)idx * BITS) &
+        const int o = (int)((ESM ? (std::uint32_t)(idx / (ESM ? ESM : 1)) * Cfg::BBB
+                             : PAD ? (std::uint32_t)(idx >> log2E) * blk_bits + (std::uint32_t)(idx & (E - 1)) * BITS
+                                   : (std::uint32_t)idx * BITS) &
                             31u);
 #pragma unroll
         for (int i = 0; i < NW; ++i) seg[i] = __funnelshift_r(wv[rr][i], wv[rr][i + 1], o);
         seg[NW] = 0;
       }
       C c[P];
-      unpack_all<0, BITS>(seg, c);
+      unpack_lane<Cfg>(seg, c);
 
       U outb[P];
-      const std::int64_t b = be[rr];
-      if (plain_exponent<T>(b)) {
-        const T inv = pow2<T>((int)b - BITS + 2);
-        const U zero_bits = sizeof(T) == 4 ? (U)((std::uint32_t)(b + 96) << 23)
-                                           : (U)((std::uint64_t)(b + 992) << 52);
+      constexpr int PB = P / NBL; // values per exponent in this lane
 #pragma unroll
-        for (int i = 0; i < P; ++i) outb[i] = decode_plain<T, BITS>(c[i], inv, zero_bits);
-      } else {
+      for (int q = 0; q < NBL; ++q) {
+        const std::int64_t b = be[rr][q];
+        if (plain_exponent<T>(b)) {
+          const T inv = pow2<T>((int)b - BITS + 2);
+          const U zero_bits = sizeof(T) == 4 ? (U)((std::uint32_t)(b + 96) << 23)
+                                             : (U)((std::uint64_t)(b + 992) << 52);
 #pragma unroll
-        for (int i = 0; i < P; ++i) outb[i] = to_bits<T>(from_code<T>((U)c[i], b, BITS));
+          for (int i = q * PB; i < (q + 1) * PB; ++i) outb[i] = decode_plain<T, BITS>(c[i], inv, zero_bits);
+        } else {
+#pragma unroll
+          for (int i = q * PB; i < (q + 1) * PB; ++i) outb[i] = to_bits<T>(from_code<T>((U)c[i], b, BITS));
+        }
       }
 
       if (full || idx + P <= rem) {
@@ -640,11 +798,11 @@ __device__ __forceinline__ void fast_decompress_tile(const Job& j, std::uint64_t
   }
 }
 
-template<class T, int BITS, int NT = kNT, int RPW = 2, bool PAD = false>
+template<class T, int BITS, int NT = kNT, int RPW = 2, bool PAD = false, int ESM = 0>
 __global__ void __launch_bounds__(NT) k_decompress_fast(Job j)
 {
   for (std::uint64_t tile = blockIdx.x; tile < j.tiles; tile += gridDim.x)
-    fast_decompress_tile<T, BITS, NT, RPW, PAD>(j, tile);
+    fast_decompress_tile<T, BITS, NT, RPW, PAD, ESM>(j, tile);
 }
 
 // Whether a job's exponent blocks end in pad bits (E * bits not a multiple of
@@ -666,7 +824,18 @@ __host__ inline bool fast_eligible(const Job& j, int dtype_is_f64, const void* v
   // segments are not word-aligned: those kernels place each lane's bits
   // by its stream position
   if (((std::uint64_t)E * (std::uint64_t)j.bits) % (std::uint64_t)j.W != 0 && (P * j.bits) % 32 == 0) return false;
-  if (dtype_is_f64 && j.bits < 8) return false;
+  if (reinterpret_cast<std::uintptr_t>(values) % 32 != 0) return false;
+  if (reinterpret_cast<std::uintptr_t>(words) % 32 != 0) return false;
+  return true;
+}
+
+// Requirements of the small-block instances (ESM = E < P values per lane):
+// E in {1, 2, 4} below the lane's P, 32-byte aligned pointers.
+__host__ inline bool small_block_eligible(const Job& j, int dtype_is_f64, const void* values, const void* words)
+{
+  const int P = dtype_is_f64 ? 4 : 8;
+  const int E = j.E;
+  if (E >= P || (E != 1 && E != 2 && E != 4)) return false;
   if (reinterpret_cast<std::uintptr_t>(values) % 32 != 0) return false;
   if (reinterpret_cast<std::uintptr_t>(words) % 32 != 0) return false;
   return true;

@@ -48,4 +48,26 @@ constexpr auto make_fast_table(std::integer_sequence<int, I...>)
 cudaError_t launch_fast_f32(int bits, bool compress, const Job& j, cudaStream_t s, unsigned grid);
 cudaError_t launch_fast_f64(int bits, bool compress, const Job& j, cudaStream_t s, unsigned grid);
 
+// Blocks of E < P values (E = 1, 2 or 4 for fp32; 1 or 2 for fp64): one
+// instance per (width, E).
+template<class T, int BITS, int ESM>
+cudaError_t launch_small_one(bool compress, const Job& j, cudaStream_t s, unsigned grid)
+{
+  if (compress)
+    k_compress_fast<T, BITS, kNT, 2, false, ESM><<<grid, kNT, 0, s>>>(j);
+  else
+    k_decompress_fast<T, BITS, kNT, 2, false, ESM><<<grid, kNT, 0, s>>>(j);
+  return cudaGetLastError();
+}
+
+template<class T, int ESM, int LO, int... I>
+constexpr auto make_small_table(std::integer_sequence<int, I...>)
+{
+  return std::array<fast_fn, sizeof...(I)>{ &launch_small_one<T, LO + I, ESM>... };
+}
+
+// Returns cudaErrorNotSupported when (bits, E) has no instance.
+cudaError_t launch_fast_small_f32(int bits, int E, bool compress, const Job& j, cudaStream_t s, unsigned grid);
+cudaError_t launch_fast_small_f64(int bits, int E, bool compress, const Job& j, cudaStream_t s, unsigned grid);
+
 } // namespace frsz2b

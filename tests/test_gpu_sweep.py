@@ -36,14 +36,18 @@ def check(x, bits, E):
 
 @pytest.mark.parametrize("bits", range(4, 33))
 def test_fp32_every_width(cuda, bits):
-    for E, n in ((32, 3 * 4096 + 77), (8, 4096 + 5), (256, 2 * 4096)):
+    for E, n in ((32, 3 * 4096 + 77), (8, 4096 + 5), (256, 2 * 4096),
+                 # blocks smaller than a lane's 8 values
+                 (4, 2 * 4096 + 5), (2, 4096 + 13), (1, 4096 + 1)):
         check(workloads.loguniform_np(n, np.float32, seed=bits * 7 + E, lo=-30, hi=30), bits, E)
 
 
 @pytest.mark.parametrize("bits", range(4, 65))
 def test_fp64_every_width(cuda, bits):
     lo, hi = (-30, 30) if bits <= 8 else (-300, 300)
-    for E, n in ((32, 3 * 2048 + 77), (4, 2048 + 3), (128, 2 * 2048 + 1)):
+    for E, n in ((32, 3 * 2048 + 77), (4, 2048 + 3), (128, 2 * 2048 + 1),
+                 # blocks smaller than a lane's 4 values
+                 (2, 2 * 2048 + 7), (1, 2048 + 5)):
         check(workloads.loguniform_np(n, np.float64, seed=bits * 11 + E, lo=lo, hi=hi), bits, E)
 
 
@@ -82,9 +86,10 @@ def special_values(dtype, n, seed):
 @pytest.mark.parametrize("dtype", [np.float32, np.float64])
 def test_special_values(cuda, dtype):
     x = special_values(dtype, 64 * 512 + 13, 5)
-    widths = (4, 8, 9, 16, 21, 24, 31, 32) if dtype == np.float32 else (8, 9, 16, 21, 32, 33, 47, 63, 64)
+    widths = (4, 8, 9, 16, 21, 24, 31, 32) if dtype == np.float32 else (4, 5, 7, 8, 9, 16, 21, 32, 33, 47, 63, 64)
+    small = (1, 2, 4) if dtype == np.float32 else (1, 2)
     for bits in widths:
-        for E in (8, 32, 64):
+        for E in (8, 32, 64) + small:
             check(x, bits, E)
 
 
