@@ -1,5 +1,6 @@
 // frsz2_capi.cu -- C ABI of libfrsz2_b200.so: argument checks, kernel choice,
 // launch geometry, and the host-buffer path with pipelined copies.
+#include "frsz2_chunked.cuh"
 #include "frsz2_fast_dispatch.hpp"
 #include "frsz2_kernels.cuh"
 #include "frsz2_launch.hpp"
@@ -131,6 +132,15 @@ static cudaError_t try_fast(bool compress, const Job& j, cudaStream_t s)
   return cudaErrorNotSupported;
 }
 
+
+// One CTA per chunk of whole blocks (frsz2_chunked.cuh).
+static unsigned chunk_grid(const Job& j)
+{
+  const std::uint64_t nb = (j.n + (std::uint64_t)j.E - 1) / (std::uint64_t)j.E;
+  const std::uint64_t nbc = (std::uint64_t)chunk_blocks(j.E);
+  return (unsigned)std::max<std::uint64_t>(1, std::min<std::uint64_t>((nb + nbc - 1) / nbc, 1u << 30));
+}
+
 template<class T>
 static int launch_compress_t(const Job& j, int dtype, cudaStream_t s, bool* used_tile)
 {
@@ -148,6 +158,8 @@ static int launch_compress_t(const Job& j, int dtype, cudaStream_t s, bool* used
       k_compress_tile<T, std::uint64_t><<<grid, kNT, compress_smem<T>(j.bits), s>>>(j);
     else
       k_compress_tile<T, std::uint32_t><<<grid, kNT, compress_smem<T>(j.bits), s>>>(j);
+  } else if (j.E <= kChunkMaxECompress) {
+    k_compress_chunked<T><<<chunk_grid(j), kNT, 0, s>>>(j);
   } else {
     const std::uint64_t nb = (j.n + (std::uint64_t)j.E - 1) / (std::uint64_t)j.E;
     k_compress_generic<T><<<grid_for(nb, kNT / 32), kNT, 0, s>>>(j);
@@ -172,6 +184,8 @@ static int launch_decompress_t(const Job& j, int dtype, cudaStream_t s, bool* us
       k_decompress_tile<T, std::uint64_t><<<grid, kNT, decompress_smem<T>(j), s>>>(j);
     else
       k_decompress_tile<T, std::uint32_t><<<grid, kNT, decompress_smem<T>(j), s>>>(j);
+  } else if (j.E <= kChunkMaxEDecompress) {
+    k_decompress_chunked<T><<<chunk_grid(j), kNT, 0, s>>>(j);
   } else {
     const std::uint64_t nb = (j.n + (std::uint64_t)j.E - 1) / (std::uint64_t)j.E;
     k_decompress_generic<T><<<grid_for(nb, kNT / 32), kNT, 0, s>>>(j);

@@ -106,3 +106,41 @@ def test_nan_inf(cuda, dtype):
     for bits in ((8, 16, 21, 32) if dtype == np.float32 else (8, 16, 21, 32, 40, 64)):
         for E in (8, 32):
             check(x, bits, E)
+
+
+@pytest.mark.parametrize("E", [3, 5, 6, 7, 12, 48, 100, 257, 1000, 2047])
+def test_block_sizes_not_powers_of_two(cuda, E):
+    """Block sizes the fast kernels do not take (chunked kernels): several
+    chunks, a partial last block, special values."""
+    for dtype, widths in ((np.float32, (4, 9, 16, 21, 32)), (np.float64, (5, 8, 21, 33, 52, 64))):
+        n = 3 * 2048 + 2 * E + E // 2 + 1
+        x = special_values(dtype, n, E)
+        for bits in widths:
+            check(x, bits, E)
+
+
+@pytest.mark.parametrize("dtype,bits,E", [(np.float32, 16, 32), (np.float32, 21, 8), (np.float64, 40, 4),
+                                          (np.float64, 21, 64), (np.float32, 13, 1)])
+def test_pointers_off_alignment(cuda, dtype, bits, E):
+    """Values and buffers at 4- and 8-byte offsets from 32-byte alignment
+    (not the fast kernels' layout): bytes and values still match the oracle,
+    bytes outside the buffer untouched."""
+    n = 2 * 4096 + 3 * E + 5
+    x = workloads.loguniform_np(n, dtype, seed=bits + E, lo=-20, hi=20)
+    es = np.dtype(dtype).itemsize
+    size = frsz_b200.compressed_size(dtype, bits, E, n)
+    w = frsz_b200.word_bits(bits) // 8  # the buffer must be word aligned
+    for voff, boff in ((1, w), (3, 3 * w), (2, 5 * w)):
+        tv = torch.zeros(n + 4, dtype=torch.float32 if dtype == np.float32 else torch.float64, device="cuda")
+        tv[voff:voff + n] = torch.from_numpy(x).cuda()
+        raw = torch.full((size + 64,), 0x5A, dtype=torch.uint8, device="cuda")
+        buf = raw[boff:boff + size]
+        frsz_b200.compress(tv[voff:voff + n], bits, E, out=buf)
+        ref = oracle.compress(x, bits, E, canary=0x5A)
+        assert np.array_equal(buf.cpu().numpy(), ref), (voff, boff)
+        assert np.all(raw[:boff].cpu().numpy() == 0x5A) and np.all(raw[boff + size:].cpu().numpy() == 0x5A)
+        y = torch.zeros_like(tv)
+        frsz_b200.decompress(buf, n, dtype, bits, E, out=y[voff:voff + n])
+        want = oracle.decompress(ref, n, dtype, bits, E)
+        uint = np.uint64 if dtype == np.float64 else np.uint32
+        assert np.array_equal(y[voff:voff + n].cpu().numpy().view(uint), want.view(uint)), (voff, boff)
