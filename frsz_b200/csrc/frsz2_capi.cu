@@ -159,7 +159,10 @@ static int launch_compress_t(const Job& j, int dtype, cudaStream_t s, bool* used
     else
       k_compress_tile<T, std::uint32_t><<<grid, kNT, compress_smem<T>(j.bits), s>>>(j);
   } else if (j.E <= kChunkMaxECompress) {
-    k_compress_chunked<T><<<chunk_grid(j), kNT, 0, s>>>(j);
+    if (j.bits <= 32)
+      k_compress_chunked<T, std::uint32_t><<<chunk_grid(j), kNT, 0, s>>>(j);
+    else
+      k_compress_chunked<T, std::uint64_t><<<chunk_grid(j), kNT, 0, s>>>(j);
   } else {
     const std::uint64_t nb = (j.n + (std::uint64_t)j.E - 1) / (std::uint64_t)j.E;
     k_compress_generic<T><<<grid_for(nb, kNT / 32), kNT, 0, s>>>(j);
@@ -185,7 +188,10 @@ static int launch_decompress_t(const Job& j, int dtype, cudaStream_t s, bool* us
     else
       k_decompress_tile<T, std::uint32_t><<<grid, kNT, decompress_smem<T>(j), s>>>(j);
   } else if (j.E <= kChunkMaxEDecompress) {
-    k_decompress_chunked<T><<<chunk_grid(j), kNT, 0, s>>>(j);
+    if (j.bits <= 32)
+      k_decompress_chunked<T, std::uint32_t><<<chunk_grid(j), kNT, 0, s>>>(j);
+    else
+      k_decompress_chunked<T, std::uint64_t><<<chunk_grid(j), kNT, 0, s>>>(j);
   } else {
     const std::uint64_t nb = (j.n + (std::uint64_t)j.E - 1) / (std::uint64_t)j.E;
     k_decompress_generic<T><<<grid_for(nb, kNT / 32), kNT, 0, s>>>(j);

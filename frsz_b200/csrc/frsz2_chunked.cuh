@@ -40,31 +40,37 @@ __device__ __forceinline__ std::uint32_t blk_record(std::int64_t be, bool plain)
 __device__ __forceinline__ std::int64_t blk_exp(std::uint32_t r) { return (std::int16_t)(r & 0xFFFFu); }
 __device__ __forceinline__ bool blk_plain(std::uint32_t r) { return (r >> 16) != 0; }
 
+// Codes are C = uint32 for bits <= 32, uint64 above (one kernel instance
+// each), so the common widths do 32-bit shifts and masks.
+
 // trunc(|x| * scale) with the sign at bit `bits` - 1 (plain domain).
-template<class T>
-__device__ __forceinline__ std::uint64_t encode_plain_rt(typename fp<T>::U u, T scale, int bits)
+template<class T, class C>
+__device__ __forceinline__ C encode_plain_rt(typename fp<T>::U u, T scale, int bits)
 {
   const T x = from_bits<T>(u);
-  const std::uint64_t s = (std::uint64_t)(u >> (fp<T>::UBITS - 1)) << (bits - 1);
+  const C s = (C)(u >> (fp<T>::UBITS - 1)) << (bits - 1);
   if constexpr (sizeof(T) == 4)
-    return (std::uint64_t)__float2uint_rz(fabsf(x) * scale) | s;
+    return (C)__float2uint_rz(fabsf(x) * scale) | s;
+  else if constexpr (sizeof(C) == 4)
+    return (C)__double2uint_rz(fabs(x) * scale) | s;
   else
-    return (bits <= 32 ? (std::uint64_t)__double2uint_rz(fabs(x) * scale) : __double2ull_rz(fabs(x) * scale)) | s;
+    return (C)__double2ull_rz(fabs(x) * scale) | s;
 }
 
 // Value of a code in the plain domain: rz(mag) * 2^(be-bits+2), a zero
 // magnitude giving 2^(be-31) (zero_bits), the code's sign bit or-ed in.
-template<class T>
-__device__ __forceinline__ typename fp<T>::U decode_plain_rt(std::uint64_t code, int bits, T inv,
-                                                             typename fp<T>::U zero_bits)
+template<class T, class C>
+__device__ __forceinline__ typename fp<T>::U decode_plain_rt(C code, int bits, T inv, typename fp<T>::U zero_bits)
 {
   using U = typename fp<T>::U;
-  const std::uint64_t mag = code & ((1ull << (bits - 1)) - 1ull);
+  const C mag = code & ((C(1) << (bits - 1)) - C(1));
   U r;
   if constexpr (sizeof(T) == 4)
     r = __float_as_uint(__uint2float_rz((std::uint32_t)mag) * inv);
+  else if constexpr (sizeof(C) == 4)
+    r = (U)__double_as_longlong(__uint2double_rn(mag) * inv);
   else
-    r = (U)__double_as_longlong((bits <= 32 ? __uint2double_rn((std::uint32_t)mag) : __ull2double_rz(mag)) * inv);
+    r = (U)__double_as_longlong(__ull2double_rz(mag) * inv);
   r = mag == 0 ? zero_bits : r;
   return r | ((U)(code >> (bits - 1)) << (fp<T>::UBITS - 1));
 }
@@ -103,7 +109,7 @@ __device__ __forceinline__ void chunk_copy(std::uint8_t* g, std::uint8_t* s, std
   }
 }
 
-template<class T>
+template<class T, class C>
 __global__ void __launch_bounds__(kNT) k_compress_chunked(Job j)
 {
   using U = typename fp<T>::U;
@@ -130,11 +136,12 @@ __global__ void __launch_bounds__(kNT) k_compress_chunked(Job j)
     const std::uint32_t hb = (std::uint32_t)(reinterpret_cast<std::uintptr_t>(gout) & 15u); // image offset
     const std::uint32_t img_words = (hb + nbk * BB + 3) / 4;
 
+    const T* __restrict__ xc = x + v0;
     U u[kChunkVPT];
 #pragma unroll
     for (int k = 0; k < kChunkVPT; ++k) {
       const int v = tid + k * kNT;
-      u[k] = v < nv ? load_bits(x + v0 + v) : U(0);
+      u[k] = v < nv ? load_bits(xc + v) : U(0);
       if (v < nv) {
         const U a = u[k] & fp<T>::ABS;
         s_key[v] = (std::uint16_t)(max_field<T>(u[k]) | (a >= fp<T>::INF ? 0x8000u : 0u));
@@ -180,26 +187,31 @@ __global__ void __launch_bounds__(kNT) k_compress_chunked(Job j)
     __syncthreads();
 
     // codes into the block image
+    const std::uint32_t bit0 = hb * 8u, bb_bits = BB * 8u;
     int b = tid / E, o = tid - (tid / E) * E;
 #pragma unroll
     for (int k = 0; k < kChunkVPT; ++k) {
       const int v = tid + k * kNT;
       if (v < nv) {
         const std::uint32_t r = s_blk[b];
-        const std::int64_t be = blk_exp(r);
-        std::uint64_t c;
+        const int be = (int)blk_exp(r);
+        C c;
         if (blk_plain(r))
-          c = encode_plain_rt<T>(u[k], pow2<T>(bits - 2 - (int)be), bits);
+          c = encode_plain_rt<T, C>(u[k], pow2<T>(bits - 2 - be), bits);
         else
-          c = (std::uint64_t)to_code<T>(u[k], (std::int16_t)be, bits);
-        const std::uint32_t pos = hb * 8u + (std::uint32_t)b * BB * 8u + (std::uint32_t)(o * bits);
+          c = (C)to_code<T>(u[k], (std::int16_t)be, bits);
+        const std::uint32_t pos = bit0 + (std::uint32_t)b * bb_bits + (std::uint32_t)(o * bits);
         const int q = (int)(pos & 31u);
         std::uint32_t* w = s_img + (pos >> 5);
         atomicOr(w, (std::uint32_t)(c << q));
         if (q + bits > 32) {
-          const std::uint64_t rest = c >> (32 - q);
-          atomicOr(w + 1, (std::uint32_t)rest);
-          if (q + bits > 64) atomicOr(w + 2, (std::uint32_t)(rest >> 32));
+          if constexpr (sizeof(C) == 4) {
+            atomicOr(w + 1, c >> (32 - q)); // q > 0 here
+          } else {
+            const std::uint64_t rest = c >> (32 - q);
+            atomicOr(w + 1, (std::uint32_t)rest);
+            if (q + bits > 64) atomicOr(w + 2, (std::uint32_t)(rest >> 32));
+          }
         }
       }
       b += step_b;
@@ -221,7 +233,7 @@ __global__ void __launch_bounds__(kNT) k_compress_chunked(Job j)
   }
 }
 
-template<class T>
+template<class T, class C>
 __global__ void __launch_bounds__(kNT) k_decompress_chunked(Job j)
 {
   using U = typename fp<T>::U;
@@ -235,7 +247,7 @@ __global__ void __launch_bounds__(kNT) k_decompress_chunked(Job j)
   const std::uint64_t nb = (j.n + (std::uint64_t)E - 1) / (std::uint64_t)E;
   const std::uint64_t nchunks = (nb + nbc - 1) / nbc;
   const int step_b = kNT / E, step_o = kNT % E;
-  const std::uint64_t cmask = bits == 64 ? ~0ull : ((1ull << bits) - 1ull);
+  const C cmask = bits == (int)(8 * sizeof(C)) ? ~C(0) : ((C(1) << bits) - C(1));
 
   for (std::uint64_t ch = blockIdx.x; ch < nchunks; ch += gridDim.x) {
     const std::uint64_t b0 = ch * (std::uint64_t)nbc;
@@ -251,30 +263,37 @@ __global__ void __launch_bounds__(kNT) k_decompress_chunked(Job j)
     if (tid < 4) s_img[(hb + nbk * BB + 3) / 4 + tid] = 0u; // words past the image read by the last codes
     __syncthreads();
 
+    const std::uint32_t bit0 = hb * 8u, bb_bits = BB * 8u;
+    T* __restrict__ yc = y + v0;
     int b = tid / E, o = tid - (tid / E) * E;
 #pragma unroll
     for (int k = 0; k < kChunkVPT; ++k) {
       const int v = tid + k * kNT;
       if (v < nv) {
-        const std::uint32_t pos = hb * 8u + (std::uint32_t)b * BB * 8u + (std::uint32_t)(o * bits);
+        const std::uint32_t pos = bit0 + (std::uint32_t)b * bb_bits + (std::uint32_t)(o * bits);
         const int q = (int)(pos & 31u);
         const std::uint32_t* w = s_img + (pos >> 5);
-        std::uint64_t c = (std::uint64_t)w[0] >> q;
-        if (q + bits > 32) {
-          c |= (std::uint64_t)w[1] << (32 - q);
-          if (q + bits > 64) c |= (std::uint64_t)w[2] << (64 - q);
+        C c;
+        if constexpr (sizeof(C) == 4) {
+          c = __funnelshift_r(w[0], w[1], q); // w[1] may be a guard word
+        } else {
+          c = (std::uint64_t)w[0] >> q;
+          if (q + bits > 32) {
+            c |= (std::uint64_t)w[1] << (32 - q);
+            if (q + bits > 64) c |= (std::uint64_t)w[2] << (64 - q);
+          }
         }
         c &= cmask;
-        const std::int64_t be = s_exp[b];
+        const int be = s_exp[b];
         U r;
         if (plain_exponent<T>(be)) {
-          const T inv = pow2<T>((int)be - bits + 2);
+          const T inv = pow2<T>(be - bits + 2);
           const U zero_bits = sizeof(T) == 4 ? (U)((std::uint32_t)(be + 96) << 23) : (U)((std::uint64_t)(be + 992) << 52);
-          r = decode_plain_rt<T>(c, bits, inv, zero_bits);
+          r = decode_plain_rt<T, C>(c, bits, inv, zero_bits);
         } else {
           r = to_bits<T>(from_code<T>((U)c, be, bits));
         }
-        y[v0 + v] = from_bits<T>(r);
+        yc[v] = from_bits<T>(r);
       }
       b += step_b;
       o += step_o;
