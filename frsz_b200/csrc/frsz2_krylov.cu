@@ -124,6 +124,105 @@ __global__ void __launch_bounds__(kKT, kMinCtas)
   }
 }
 
+// Dot with work handed out at run time: an item is a group of vg vectors over
+// a slice of kSub values; CTAs take items from a counter in the workspace, so
+// SMs that run slower take fewer (a fixed split measured a 10 % spread of SM
+// busy time), and write each (vector, slice) sum to its own place in
+// partials; k_basis_dot_final adds them in slice order, so h does not depend
+// on which CTA took which item, on the grid or on vg.
+template<int BITS>
+__global__ void __launch_bounds__(kKT, kMinCtas)
+  k_basis_dot_dyn(const __grid_constant__ BasisParams bp, int m, BasisGeo g, const double* __restrict__ w,
+                  unsigned int ns, int vg, double* __restrict__ partials, unsigned int* __restrict__ next_item)
+{
+  constexpr int P = fast_cfg<double, BITS>::P;
+  __shared__ double s_w[kSub];
+  __shared__ double s_acc[kKT / 32][kMaxBasis];
+  __shared__ unsigned int s_item;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const unsigned int groups = (unsigned)((m + vg - 1) / vg);
+  const unsigned int items = ns * groups;
+
+  for (;;) {
+    if (tid == 0) s_item = atomicAdd(next_item, 1u);
+    __syncthreads(); // also: the previous item's s_w / s_acc are consumed
+    const unsigned int it = s_item;
+    if (it >= items) break;
+    // an item: vectors [jb, je) over slice sl
+    const unsigned int sl = it / groups;
+    const int jb = (int)(it - sl * groups) * vg, je = min(jb + vg, m);
+    const std::uint64_t s0 = (std::uint64_t)sl * kSub;
+    const int len = (int)((g.n - s0) < (std::uint64_t)kSub ? (g.n - s0) : (std::uint64_t)kSub);
+    for (int i = tid; i < len; i += kKT) s_w[i] = __ldg(w + s0 + i);
+    __syncthreads();
+    // kJB vectors at a time: all their loads are issued before any decode
+    for (int j0 = jb; j0 < je; j0 += kJB) {
+      double acc[kJB];
+#pragma unroll
+      for (int jj = 0; jj < kJB; ++jj) acc[jj] = 0.0;
+      for (int i = tid * P; i < len; i += kKT * P) {
+        lane_words<double, BITS> lw[kJB];
+#pragma unroll
+        for (int jj = 0; jj < kJB; ++jj)
+          if (j0 + jj < je) {
+            const std::uint8_t* buf = bp.buf[j0 + jj];
+            fast_load_lane<double, BITS>(buf, buf + g.exp_bytes, g.log2E, s0 + (std::uint64_t)i, lw[jj]);
+          }
+        double wv[P];
+#pragma unroll
+        for (int k = 0; k < P; ++k) wv[k] = i + k < len ? s_w[i + k] : 0.0;
+#pragma unroll
+        for (int jj = 0; jj < kJB; ++jj)
+          if (j0 + jj < je) {
+            double v[P];
+            fast_decode_loaded<double, BITS>(lw[jj], v);
+#pragma unroll
+            for (int k = 0; k < P; ++k) acc[jj] = fma(v[k], wv[k], acc[jj]);
+          }
+      }
+#pragma unroll
+      for (int jj = 0; jj < kJB; ++jj) {
+        double a = acc[jj];
+#pragma unroll
+        for (int sh = 16; sh > 0; sh >>= 1) a += __shfl_down_sync(0xFFFFFFFFu, a, sh);
+        if (lane == 0 && j0 + jj < je) s_acc[warp][j0 + jj] = a; // each (warp, vector) once per item
+      }
+    }
+    __syncthreads();
+    // this item's sums, vector-major: partials[j * ns + sl]
+    for (int j = jb + tid; j < je; j += kKT) {
+      double p = 0.0;
+#pragma unroll
+      for (int q = 0; q < kKT / 32; ++q) p += s_acc[q][j];
+      partials[(std::uint64_t)j * ns + sl] = p;
+    }
+  }
+}
+
+// h[j] = sum over slices of partials[j * ns + slice], in a fixed order; one
+// CTA per vector.  Leaves the slice counter at zero for the next call.
+__global__ void __launch_bounds__(kKT)
+  k_basis_dot_final(const double* __restrict__ partials, unsigned int ns, double* __restrict__ h,
+                    unsigned int* __restrict__ next_slice)
+{
+  __shared__ double s_red[kKT / 32];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const double* pj = partials + (std::uint64_t)blockIdx.x * ns;
+  double sum = 0.0;
+  for (unsigned int b = tid; b < ns; b += kKT) sum += __ldcg(pj + b);
+#pragma unroll
+  for (int sh = 16; sh > 0; sh >>= 1) sum += __shfl_down_sync(0xFFFFFFFFu, sum, sh);
+  if (lane == 0) s_red[warp] = sum;
+  __syncthreads();
+  if (tid == 0) {
+    double t = 0.0;
+#pragma unroll
+    for (int q = 0; q < kKT / 32; ++q) t += s_red[q];
+    h[blockIdx.x] = t;
+    if (blockIdx.x == 0) *next_slice = 0u;
+  }
+}
+
 template<int BITS>
 __global__ void __launch_bounds__(kKT, kMinCtas)
   k_basis_axpy(const __grid_constant__ BasisParams bp, int m, BasisGeo g, const double* __restrict__ coef,
@@ -222,6 +321,20 @@ std::uint64_t dot_chunk(std::uint64_t n, std::uint64_t ctas)
   return std::max<std::uint64_t>(256, ((chunk + 255) / 256) * 256);
 }
 
+#ifndef FRSZ2_KRYLOV_DYNAMIC
+#define FRSZ2_KRYLOV_DYNAMIC 1
+#endif
+
+template<int BITS>
+int dyn_ctas_per_sm()
+{
+  int blocks = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k_basis_dot_dyn<BITS>, kKT, 0) != cudaSuccess ||
+      blocks < 1)
+    blocks = 1;
+  return std::min(blocks, kMaxCtasPerSm);
+}
+
 template<int BITS>
 int dot_ctas_per_sm()
 {
@@ -240,10 +353,10 @@ extern "C" {
 
 uint64_t frsz2_basis_workspace_size(int m, uint64_t n)
 {
-  (void)n;
   if (m < 0) m = 0;
   const std::uint64_t grid = (std::uint64_t)sm_count() * kMaxCtasPerSm;
-  return 256 + grid * (std::uint64_t)std::max(m, 1) * sizeof(double);
+  const std::uint64_t slices = (n + kSub - 1) / kSub; // one row of m sums per slice
+  return 256 + std::max(grid, slices) * (std::uint64_t)std::max(m, 1) * sizeof(double);
 }
 
 int frsz2_basis_dot(int dtype, int bits, int block_size, const void* const* basis, int m, uint64_t n,
@@ -261,6 +374,47 @@ int frsz2_basis_dot(int dtype, int bits, int block_size, const void* const* basi
     return set_error(FRSZ2_EFAIL, "workspace must be 256-byte aligned");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   if (n == 0) return cuda_status(cudaMemsetAsync(h, 0, (std::size_t)m * sizeof(double), s), "memset");
+  if (FRSZ2_KRYLOV_DYNAMIC) {
+    const std::uint64_t ns64 = (n + kSub - 1) / kSub;
+    if (ns64 > 0xFFFFFFFFull) return set_error(FRSZ2_EFAIL, "basis vectors too long");
+    const unsigned ns = (unsigned)ns64;
+    auto* next_slice = static_cast<unsigned int*>(workspace);
+    auto* rows = reinterpret_cast<double*>(static_cast<std::uint8_t*>(workspace) + 256);
+    int per = 1;
+    switch (bits) {
+#define CASE(B)                                                                                                    \
+  case B: per = dyn_ctas_per_sm<B>(); break;
+      FRSZ2_KRYLOV_WIDTHS(CASE)
+#undef CASE
+    }
+    const std::uint64_t ctas = (std::uint64_t)sm_count() * (std::uint64_t)per;
+    // vectors per item: up to 32 vectors, all of them (whole slices); more,
+    // about 8 items per CTA in multiples of kJB and at least 16 vectors (each
+    // item stages its slice of w once).  Measured on B200 with 2^22-value
+    // vectors, 32 bits: m = 100 0.76 of HBM with 32 vectors per item against
+    // 0.74 with whole slices; m = 20 0.67 with whole slices against 0.62 with
+    // 16 per item.
+    std::uint64_t vg = (std::uint64_t)m;
+    if (m > 32) {
+      vg = ((std::uint64_t)m * ns + 8 * ctas - 1) / (8 * ctas);
+      vg = std::min<std::uint64_t>((std::uint64_t)m, std::max<std::uint64_t>(16, (vg + kJB - 1) / kJB * kJB));
+    }
+    const std::uint64_t items = ns * (((std::uint64_t)m + vg - 1) / vg);
+    if (items > 0xFFFFFFFFull) return set_error(FRSZ2_EFAIL, "basis vectors too long");
+    const unsigned grid = (unsigned)std::max<std::uint64_t>(1, std::min<std::uint64_t>(items, ctas));
+    switch (bits) {
+#define CASE(B)                                                                                                    \
+  case B:                                                                                                          \
+    k_basis_dot_dyn<B><<<grid, kKT, 0, s>>>(bp, m, g, static_cast<const double*>(w), ns, (int)vg, rows,          \
+                                            next_slice);                                                           \
+    break;
+      FRSZ2_KRYLOV_WIDTHS(CASE)
+#undef CASE
+    }
+    if (int rc = cuda_status(cudaGetLastError(), "basis dot launch")) return rc;
+    k_basis_dot_final<<<(unsigned)m, kKT, 0, s>>>(rows, ns, static_cast<double*>(h), next_slice);
+    return cuda_status(cudaGetLastError(), "basis dot launch");
+  }
   int per_sm = 1;
   switch (bits) {
 #define CASE(B)                                                                                                    \

@@ -186,9 +186,10 @@ int frsz2_batch_compress_static(const frsz2_batch_item* items, uint64_t count, v
  * sizes that are powers of two without block padding; m <= FRSZ2_MAX_BASIS.
  *
  * frsz2_basis_dot:  h[j] = sum_i V_j[i] * w[i], j < m.  `workspace` is device
- *   memory of frsz2_basis_workspace_size(m, n) bytes, 256-byte aligned, zero
- *   on first use (the call leaves it ready for the next one); the result does
- *   not depend on scheduling.  Calls sharing a workspace must not overlap.
+ *   memory of frsz2_basis_workspace_size(m, n) bytes (m sums per slice of
+ *   3,072 values), 256-byte aligned, zero on first use (the call leaves it
+ *   ready for the next one); the result does not depend on scheduling.  Calls
+ *   sharing a workspace must not overlap.
  * frsz2_basis_axpy: y[i] += sum_j c[j] * V_j[i] (j in order), c and y device
  *   memory, y 32-byte aligned.
  */
