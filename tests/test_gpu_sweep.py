@@ -73,8 +73,9 @@ def special_values(dtype, n, seed):
             x[sl] = (rng.standard_normal(B) * float(fi.tiny) * 2 ** rng.integers(0, 40)).astype(dtype)
         elif kind == 1:  # only subnormals and zeros
             x[sl] = (rng.random(B) * float(fi.tiny)).astype(dtype) * (rng.random(B) < 0.7)
-        elif kind == 2:  # near the top of the range
-            x[sl] = (rng.standard_normal(B) * float(fi.max) / 4).astype(dtype)
+        elif kind == 2:  # near the top of the range (the largest overflow to +-Inf)
+            with np.errstate(over="ignore"):
+                x[sl] = (rng.standard_normal(B) * float(fi.max) / 4).astype(dtype)
         elif kind == 3:  # signed zeros
             x[sl] = np.where(rng.random(B) < 0.5, -0.0, 0.0).astype(dtype)
         else:            # exponent boundary of the plain range
