@@ -72,6 +72,9 @@ SIGNATURES = {
     "frsz2_decompress_host": (_int, [_int, _int, _int, _vp, _u64, _vp, _vp]),
     "frsz2_decompress_elements": (_int, [_int, _int, _int, _vp, _u64, _vp, _u64, _vp, _vp]),
     "frsz2_decompress_elements_host": (_int, [_int, _int, _int, _vp, _u64, _vp, _u64, _vp]),
+    "frsz1_compressed_size": (_u64, [_u64]),
+    "frsz1_compress": (_int, [_int, ctypes.c_double, _vp, _u64, _vp, _vp]),
+    "frsz1_decompress": (_int, [_int, ctypes.c_double, _vp, _u64, _vp, _int, _vp]),
     "frsz2_compress_blocks": (_int, [_int, _int, _int, _vp, _u64, _u64, _u64, _vp, _vp]),
     "frsz2_decompress_blocks": (_int, [_int, _int, _int, _vp, _u64, _u64, _u64, _vp, _vp]),
     "frsz2_batch_create": (_int, [ctypes.POINTER(BatchItemC), _u64, ctypes.POINTER(_vp)]),

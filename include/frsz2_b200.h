@@ -262,6 +262,26 @@ int frsz2_server_release(frsz2_server* server, uint64_t id);
 int frsz2_server_stats(frsz2_server* server, frsz2_server_counters* stats);
 void frsz2_server_destroy(frsz2_server* server);
 
+/* ---------------------------------------------------------------------------
+ * The reference's legacy "frsz" codec (the LibPressio plugin "frsz",
+ * src/frsz.cc:15-165): values quantized with step 2*epsilon and stored as
+ * int16 differences to the previous quantized value within blocks of 256
+ * values; frsz1_compressed_size(n) = 2n bytes.  Device buffers,
+ * stream-ordered.  compress / decompress follow compress_1d / decompress_1d
+ * (src/frsz.cc:103-150) bit for bit; a NaN difference, undefined there, is
+ * stored as 0.  dtype FRSZ2_FLOAT / FRSZ2_DOUBLE (else FRSZ2_EDTYPE with the
+ * reference's message), epsilon > 0 (the plugin's "frsz:epsilon", default
+ * 1e-4).  decompress as the reference adds block 0's differences in every
+ * block (its decompress_1d reads quantized[i] with i the index within the
+ * block); flags FRSZ1_OWN_DELTAS adds each block's own, the inverse of
+ * compress.
+ */
+#define FRSZ1_OWN_DELTAS 1
+uint64_t frsz1_compressed_size(uint64_t n);
+int frsz1_compress(int dtype, double epsilon, const void* d_values, uint64_t n, void* d_out, void* stream);
+int frsz1_decompress(int dtype, double epsilon, const void* d_compressed, uint64_t n, void* d_values, int flags,
+                     void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -83,6 +83,11 @@ def oracle_lib():
             getattr(lib, f"frsz2o_decompress_element_{t}").restype = ft
         lib.frsz2o_compress_mt.argtypes = [ctypes.c_int, _vp, _c_size, ctypes.c_int, ctypes.c_int, _vp, ctypes.c_int]
         lib.frsz2o_decompress_mt.argtypes = [ctypes.c_int, _vp, _c_size, ctypes.c_int, ctypes.c_int, _vp, ctypes.c_int]
+        for t in ("f32", "f64"):
+            getattr(lib, f"frsz1o_compress_{t}").argtypes = [_vp, _c_size, ctypes.c_double, _vp]
+            getattr(lib, f"frsz1o_compress_{t}").restype = None
+            getattr(lib, f"frsz1o_decompress_{t}").argtypes = [_vp, _c_size, ctypes.c_double, ctypes.c_int, _vp]
+            getattr(lib, f"frsz1o_decompress_{t}").restype = None
         _oracle = lib
     return _oracle
 
@@ -241,3 +246,25 @@ def error_bound(block_exponents: np.ndarray, bits: int) -> np.ndarray:
     frsz2.hpp:361-370, and uint_fp_to_compressed, frsz2.hpp:555-558)."""
     e = block_exponents.astype(np.float64)
     return np.maximum(np.exp2(e - bits + 2), np.exp2(e - 31))
+
+
+# ---------------------------------------------------------------- legacy "frsz"
+
+def frsz1_compress(x: np.ndarray, epsilon: float) -> np.ndarray:
+    """The legacy codec's int16 stream of x (src/frsz.cc:103-130)."""
+    x = np.ascontiguousarray(x)
+    out = np.empty(x.size, dtype=np.int16)
+    t = "f64" if x.dtype == np.float64 else "f32"
+    getattr(oracle_lib(), f"frsz1o_compress_{t}")(_np_ptr(x), x.size, float(epsilon), _np_ptr(out))
+    return out
+
+
+def frsz1_decompress(q: np.ndarray, dtype, epsilon: float, own_deltas: bool = False) -> np.ndarray:
+    """The legacy codec's values from its int16 stream (src/frsz.cc:132-150);
+    own_deltas=False reproduces the reference's use of block 0's deltas."""
+    q = np.ascontiguousarray(q, dtype=np.int16)
+    out = np.empty(q.size, dtype=dtype)
+    t = "f64" if np.dtype(dtype) == np.float64 else "f32"
+    getattr(oracle_lib(), f"frsz1o_decompress_{t}")(_np_ptr(q), q.size, float(epsilon), int(own_deltas),
+                                                   _np_ptr(out))
+    return out

@@ -1,0 +1,102 @@
+"""The legacy "frsz" codec (src/frsz.cc:15-165): the oracle against the
+reference test's known answer (test/test_frsz.cc:29-46) on CPU, and the CUDA
+kernels against the oracle, bit for bit, on the GPU -- int16 streams and
+decoded values, in both decode modes (the reference's use of block 0's
+differences, and each block's own)."""
+import numpy as np
+import pytest
+import torch
+
+import oracle
+import frsz_b200
+from frsz_b200 import legacy, workloads
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_oracle_reference_known_answer(dtype):
+    # test/test_frsz.cc:29-46: epsilon 5, {10, 20, 30, 20, 10} round trips
+    x = np.array([10.0, 20.0, 30.0, 20.0, 10.0], dtype=dtype)
+    q = oracle.frsz1_compress(x, 5.0)
+    assert q.tolist() == [1, 1, 1, -1, -1]
+    assert np.array_equal(oracle.frsz1_decompress(q, dtype, 5.0), x)
+
+
+def test_oracle_block_rules():
+    # differences restart every 256 values; saturation at the int16 limits;
+    # the reference decoder adds block 0's differences in later blocks
+    x = np.arange(600, dtype=np.float64) * 2.0
+    q = oracle.frsz1_compress(x, 0.5)  # step 1: quantized values 0, 2, 4, ...
+    assert q[0] == 0 and q[256] == 512 and q[512] == 1024 and np.all(q[1:256] == 2)
+    # differences: 5e8, -1e9, +Inf (Inf - -5e8), NaN (NaN - Inf)
+    big = oracle.frsz1_compress(np.array([1e9, -1e9, np.inf, np.nan], dtype=np.float32), 1.0)
+    assert big.tolist() == [32767, -32768, 32767, 0]
+    y_ref = oracle.frsz1_decompress(q, np.float64, 0.5)
+    y_own = oracle.frsz1_decompress(q, np.float64, 0.5, own_deltas=True)
+    assert np.array_equal(y_own, x)
+    assert np.array_equal(y_ref[:256], x[:256])
+    # block 1 starts from its own first value, then adds block 0's differences
+    assert y_ref[256] == x[256] and y_ref[257] == x[256] + 2.0
+
+
+def test_plugin_options():
+    p = legacy.Frsz1Plugin()
+    assert p.get_options() == {"frsz:epsilon": 1e-4}
+    p.set_options({"frsz:epsilon": 0.25})
+    assert p.epsilon == 0.25
+
+
+def cases():
+    rng = np.random.default_rng(5)
+    out = []
+    for dtype in (np.float32, np.float64):
+        for n in (1, 7, 255, 256, 257, 1000, 65_536 + 13, (1 << 20) + 5):
+            for eps in (1e-4, 0.5, 1e-7):
+                x = workloads.normal_np(n, dtype, seed=n % 97) * dtype(10.0)
+                if n > 10:
+                    k = max(1, n // 200)
+                    idx = rng.integers(0, n, (5, k))
+                    x[idx[0]] = np.nan
+                    x[idx[1]] = np.inf
+                    x[idx[2]] = -np.inf
+                    x[idx[3]] = -0.0
+                    x[idx[4]] = dtype(3e8)
+                out.append((x, eps))
+    return out
+
+
+@pytest.mark.gpu
+def test_gpu_equals_oracle(cuda):
+    for x, eps in cases():
+        t = torch.from_numpy(x).cuda()
+        q = legacy.compress(t, eps)
+        want = oracle.frsz1_compress(x, eps)
+        assert np.array_equal(q.cpu().numpy(), want), (x.dtype, x.size, eps)
+        uint = np.uint64 if x.dtype == np.float64 else np.uint32
+        for own in (False, True):
+            y = legacy.decompress(torch.from_numpy(want).cuda(), t.dtype, eps, own_deltas=own).cpu().numpy()
+            yw = oracle.frsz1_decompress(want, x.dtype, eps, own_deltas=own)
+            assert np.array_equal(y.view(uint), yw.view(uint)), (x.dtype, x.size, eps, own)
+
+
+@pytest.mark.gpu
+def test_gpu_reference_known_answer_and_errors(cuda):
+    x = torch.tensor([10.0, 20.0, 30.0, 20.0, 10.0], device="cuda")
+    q = legacy.compress(x, 5.0)
+    assert q.cpu().tolist() == [1, 1, 1, -1, -1]
+    assert torch.equal(legacy.decompress(q, torch.float32, 5.0), x)
+    lib = frsz_b200.lib()
+    assert lib.frsz1_compressed_size(1000) == 2000
+    assert lib.frsz1_compress(7, 1.0, x.data_ptr(), 5, q.data_ptr(), None) == frsz_b200.FRSZ2_EDTYPE
+    assert b"only floating point" in lib.frsz2_last_error()
+    assert lib.frsz1_compress(0, 0.0, x.data_ptr(), 5, q.data_ptr(), None) == frsz_b200.FRSZ2_EFAIL
+
+
+@pytest.mark.gpu
+def test_gpu_pointers_off_vector_alignment(cuda):
+    n = 10_003
+    x = workloads.normal_np(n, np.float32, seed=3)
+    base = torch.zeros(n + 3, dtype=torch.float32, device="cuda")
+    base[1:1 + n] = torch.from_numpy(x).cuda()
+    out = torch.zeros(n + 3, dtype=torch.int16, device="cuda")
+    q = legacy.compress(base[1:1 + n], 0.01, out=out[1:1 + n])
+    assert np.array_equal(q.cpu().numpy(), oracle.frsz1_compress(x, 0.01))
