@@ -53,9 +53,19 @@ WORKLOADS = {
     # smaller cases (still larger than L2) for ncu captures
     "loguniform_f64_2p25_b21_e32": ("loguniform", "float64", 1 << 25, 21, 32),
     "loguniform_f64_2p25_b16_e64": ("loguniform", "float64", 1 << 25, 16, 64),
+    # kernel families off the default path: blocks of fewer values than a lane,
+    # padded blocks, fp64 below 8 bits, block sizes that are not powers of two
+    "normal_f32_2p28_b16_e2": ("normal", "float32", 1 << 28, 16, 2),
+    "normal_f64_2p27_b33_e32": ("normal", "float64", 1 << 27, 33, 32),
+    "normal_f64_2p27_b5_e32": ("normal", "float64", 1 << 27, 5, 32),
+    "normal_f32_2p28_b16_e5": ("normal", "float32", 1 << 28, 16, 5),
+    "normal_f32_2p25_b16_e2": ("normal", "float32", 1 << 25, 16, 2),
+    "normal_f64_2p24_b33_e32": ("normal", "float64", 1 << 24, 33, 32),
+    "normal_f64_2p24_b5_e32": ("normal", "float64", 1 << 24, 5, 32),
+    "normal_f32_2p25_b16_e5": ("normal", "float32", 1 << 25, 16, 5),
 }
 DEFAULT_WORKLOAD = "field512_f32_b16_e32"
-BATCH_WORKLOADS = ("batched4096", "krylov100", "serving")
+BATCH_WORKLOADS = ("batched4096", "krylov100", "serving", "legacy_f32_2p28", "legacy_f64_2p27", "legacy_f32_2p25")
 
 # DRAM bytes (read + write) per launch from ncu captures, by (workload, kernel);
 # profiles/ holds the captures' summaries and the commands that made them.
@@ -768,6 +778,51 @@ def run_serving(args, rank: int, world: int, local_rank: int) -> None:
     print(json.dumps(line), flush=True)
 
 
+def run_legacy(args, rank: int, world: int, local_rank: int) -> None:
+    """The legacy "frsz" codec (src/frsz.cc) on N(0,1) data, epsilon 1e-3:
+    compress, then decompress as the reference does and with each block's
+    own differences.  Bytes per launch: the values plus the int16 stream."""
+    import torch
+
+    from frsz_b200 import legacy
+
+    torch.cuda.set_device(local_rank)
+    dtype = torch.float32 if "_f32_" in args.workload else torch.float64
+    n = 1 << int(args.workload.rsplit("2p", 1)[1])
+    g = torch.Generator(device="cuda").manual_seed(args.seed + rank)
+    x = torch.randn(n, generator=g, device="cuda", dtype=dtype)
+    q = torch.empty(n, dtype=torch.int16, device="cuda")
+    y = torch.empty_like(x)
+    stream = torch.cuda.current_stream()
+
+    def timed(fn):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(args.steps):
+            fn()
+        b.record(stream)
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / args.steps
+
+    ms_c = timed(lambda: legacy.compress(x, 1e-3, out=q))
+    ms_d = timed(lambda: legacy.decompress(q, dtype, 1e-3, out=y))
+    ms_o = timed(lambda: legacy.decompress(q, dtype, 1e-3, own_deltas=True, out=y))
+    nbytes = n * (x.element_size() + 2)
+    peak = load_peaks()["hbm_gbs"]
+    gbs = [nbytes / ms / 1e6 for ms in (ms_c, ms_d, ms_o)]
+    if rank == 0:
+        print(json.dumps({"metric": "legacy frsz compress / decompress GB/s", "value": round(gbs[0], 1), "unit": "GB/s",
+                          "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+                          "dtype": str(dtype).replace("torch.", ""), "data": "synthetic N(0,1), epsilon 1e-3",
+                          "config": {"workload": args.workload, "n": n},
+                          "compress_gbs": round(gbs[0], 1), "decompress_reference_gbs": round(gbs[1], 1),
+                          "decompress_own_deltas_gbs": round(gbs[2], 1),
+                          "hbm_frac": [round(v / peak, 3) for v in gbs]}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
     ap.add_argument("--gpus", type=int, default=1)
@@ -799,6 +854,8 @@ def main():
         run_krylov(args, rank, world, local_rank)
     elif args.workload == "serving":
         run_serving(args, rank, world, local_rank)
+    elif args.workload.startswith("legacy_"):
+        run_legacy(args, rank, world, local_rank)
     elif args.impl == "reference":
         run_reference_arm(args, rank, world)
     else:
