@@ -401,9 +401,11 @@ __device__ __forceinline__ void load_lane_exps(const std::uint8_t* p, std::int64
 // One tile of compress.  s_rmax: 2 * Cfg::ROWS words of shared memory (used
 // only when an exponent block spans several warp rows); s_stage:
 // stage_words<>::value words, 16-byte aligned.
+// more_tiles: whether the CTA runs another tile after this one (the shared
+// block maxima are then reused, so their readers must be done first).
 template<class T, int BITS, int NT, int RPW_, bool PAD = false, int ESM = 0>
 __device__ __forceinline__ void fast_compress_tile(const Job& j, std::uint64_t tile, std::uint32_t* s_rmax,
-                                                   std::uint32_t* s_stage)
+                                                   std::uint32_t* s_stage, bool more_tiles = true)
 {
   using Cfg = fast_cfg<T, BITS, NT, RPW_, ESM>;
   using U = typename Cfg::U;
@@ -508,7 +510,7 @@ __device__ __forceinline__ void fast_compress_tile(const Job& j, std::uint64_t t
         km[rr] = a;
         kc[rr] = b;
       }
-      __syncthreads();
+      if (more_tiles) __syncthreads();
     }
     }
 
@@ -676,7 +678,7 @@ __global__ void __launch_bounds__(NT) k_compress_fast(Job j)
   __shared__ std::uint32_t s_rmax[2 * fast_cfg<T, BITS, NT, RPW>::ROWS];
   __shared__ __align__(16) std::uint32_t s_stage[stage_words<T, BITS, NT, RPW, ESM>::value];
   for (std::uint64_t tile = blockIdx.x; tile < j.tiles; tile += gridDim.x)
-    fast_compress_tile<T, BITS, NT, RPW, PAD, ESM>(j, tile, s_rmax, s_stage);
+    fast_compress_tile<T, BITS, NT, RPW, PAD, ESM>(j, tile, s_rmax, s_stage, tile + gridDim.x < j.tiles);
 }
 
 // ---------------------------------------------------------------- decompress
