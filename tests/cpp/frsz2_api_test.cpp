@@ -1,11 +1,13 @@
 // C++ API test: the reference-shaped template API (frsz2_b200.hpp) and the
-// plugin front end (frsz2_b200_plugin.hpp) over libfrsz2_b200.so.
+// plugin front ends (frsz2_b200_plugin.hpp, frsz1_b200_plugin.hpp) over
+// libfrsz2_b200.so.
 //
 // Usage: frsz2_api_test <out.bin>
 // Writes, for each of the reference GPU test's end-to-end cases
 // (test/test_frsz_gpu.cu:382-410), the 0xFF-canary buffer (+128 slack)
 // produced by compress_cpu_impl, so the caller can compare it with the
 // reference's bytes.  Exits non-zero on any failed check.
+#include "frsz1_b200_plugin.hpp"
 #include "frsz2_b200.hpp"
 #include "frsz2_b200_plugin.hpp"
 
@@ -152,6 +154,65 @@ static void plugin_checks()
   CHECK((p.compress(in, comp) == 2 && p.error_msg() == "Unsupported number of bits: 40"));
 }
 
+// The legacy "frsz" plugin: the reference test's known answer
+// (test/test_frsz.cc:29-46), the block rules of compress_1d / decompress_1d
+// (src/frsz.cc:105-158), the normalized_dims length rule, device data and the
+// error surface.
+static void legacy_plugin_checks()
+{
+  using frsz2_b200::data_view;
+  using frsz2_b200::dtype;
+  frsz2_b200::frsz_plugin p;
+  CHECK(p.get_options().at("frsz:epsilon") == 1e-4);
+  CHECK(std::string(p.prefix()) == "frsz" && std::string(p.version()) == "0.0.6" && p.patch_version() == 6);
+  CHECK(p.get_configuration().at("pressio:stability") == "experimental");
+  CHECK(p.get_documentation().at("pressio:description") == "a fixed rate version of the SZ Algorithm");
+  p.set_options({ { "frsz:epsilon", 5.0 } });
+  std::vector<float> f{ 10.f, 20.f, 30.f, 20.f, 10.f };
+  data_view in{ dtype::float32, f.data(), { f.size() }, false };
+  std::vector<std::uint8_t> comp;
+  CHECK(p.compress(in, comp) == 0 && comp.size() == 10);
+  std::int16_t q[5];
+  std::memcpy(q, comp.data(), 10);
+  CHECK(q[0] == 1 && q[1] == 1 && q[2] == 1 && q[3] == -1 && q[4] == -1);
+  std::vector<float> g(5, -1.f);
+  data_view out{ dtype::float32, g.data(), { 5 }, false };
+  CHECK(p.decompress(comp.data(), comp.size(), out) == 0 && g == f);
+
+  // 600 doubles 0, 2, 4, ... with step 1: block 1's first value is its own,
+  // then the reference adds block 0's differences (2 each)
+  p.set_options({ { "frsz:epsilon", 0.5 } });
+  std::vector<double> x(600);
+  for (std::size_t i = 0; i < x.size(); ++i) x[i] = 2.0 * (double)i;
+  void* dx = nullptr;
+  void* dy = nullptr;
+  CHECK(cudaMalloc(&dx, 600 * 8) == cudaSuccess && cudaMalloc(&dy, 600 * 8) == cudaSuccess);
+  CHECK(cudaMemcpy(dx, x.data(), 600 * 8, cudaMemcpyHostToDevice) == cudaSuccess);
+  data_view din{ dtype::float64, dx, { 600 }, true };
+  CHECK(p.compress(din, comp) == 0 && comp.size() == 1200);
+  std::vector<std::int16_t> d(600);
+  std::memcpy(d.data(), comp.data(), 1200);
+  CHECK(d[0] == 0 && d[1] == 2 && d[255] == 2 && d[256] == 512 && d[512] == 1024);
+  data_view dout{ dtype::float64, dy, { 600 }, true };
+  CHECK(p.decompress(comp.data(), comp.size(), dout) == 0);
+  std::vector<double> y(600);
+  CHECK(cudaMemcpy(y.data(), dy, 600 * 8, cudaMemcpyDeviceToHost) == cudaSuccess);
+  CHECK(y[255] == x[255] && y[256] == x[256] && y[257] == x[256] + 2.0 && y[599] == x[512] + 2.0 * 87);
+  cudaFree(dx);
+  cudaFree(dy);
+
+  // a 2-D array codes its first extent only; a single value codes none
+  std::vector<float> h(2160, 3.0f);
+  data_view in2{ dtype::float32, h.data(), { 40, 54 }, false };
+  CHECK(p.compress(in2, comp) == 0 && comp.size() == 80);
+  data_view one{ dtype::float32, h.data(), { 1 }, false };
+  CHECK(p.compress(one, comp) == 0 && comp.empty());
+
+  data_view bad{ dtype::other, h.data(), { 10 }, false };
+  CHECK((p.compress(bad, comp) == 1 && p.error_msg() == "unsupported type: currently only floating point supported"));
+  CHECK(p.decompress(comp.data(), 0, out) == 2);
+}
+
 int main(int argc, char** argv)
 {
   register_frsz();
@@ -171,6 +232,7 @@ int main(int argc, char** argv)
   std::fclose(out);
   dispatch_checks();
   plugin_checks();
+  legacy_plugin_checks();
   std::printf("%s (%d failures)\n", failures ? "FAILED" : "OK", failures);
   return failures ? 1 : 0;
 }

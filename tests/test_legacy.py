@@ -38,11 +38,38 @@ def test_oracle_block_rules():
     assert y_ref[256] == x[256] and y_ref[257] == x[256] + 2.0
 
 
-def test_plugin_options():
+def test_plugin_surface():
+    # src/frsz.cc:19-46, 82-86, 160; CMakeLists.txt:3 (project version)
     p = legacy.Frsz1Plugin()
     assert p.get_options() == {"frsz:epsilon": 1e-4}
     p.set_options({"frsz:epsilon": 0.25})
-    assert p.epsilon == 0.25
+    assert p.epsilon == 0.25 and p.clone().get_options() == {"frsz:epsilon": 0.25}
+    assert p.get_configuration() == {"pressio:thread_safe": "multiple", "pressio:stability": "experimental"}
+    doc = p.get_documentation()
+    assert doc["pressio:description"] == "a fixed rate version of the SZ Algorithm"
+    assert doc["frsz:epsilon"].startswith('"absolute error bound" applied during quantization')
+    assert (p.prefix, p.version(), p.major_version(), p.minor_version(), p.patch_version()) == ("frsz", "0.0.6", 0, 0, 6)
+    assert p.get_metrics_results() == {}
+    msg = "unsupported type: currently only floating point supported"
+    assert p.compress(np.zeros(4, dtype=np.int32)) == (1, None) and (p.error_code, p.error_msg) == (1, msg)
+    assert p.decompress(np.zeros(8, dtype=np.uint8), np.zeros(4, dtype=np.float16)) == 1
+
+
+def test_plugin_length_rule():
+    # normalized_dims(1).at(0) (src/frsz.cc:108, 139): unit extents dropped,
+    # the first one left is the length, 0 when none is left
+    assert legacy.legacy_length((1000,)) == 1000
+    assert legacy.legacy_length((40, 54)) == 40
+    assert legacy.legacy_length((1, 1, 7, 3)) == 7
+    assert legacy.legacy_length((1,)) == 0 and legacy.legacy_length(()) == 0
+    p = legacy.Frsz1Plugin()
+    # nothing to code: no device work, an empty stream, the output untouched
+    rc, buf = p.compress(np.ones((1, 1), dtype=np.float32))
+    assert rc == 0 and buf.size == 0
+    y = np.full(1, 7.0)
+    assert p.decompress(buf, y) == 0 and y[0] == 7.0
+    assert p.decompress(np.zeros(3, dtype=np.uint8), np.zeros(2)) == 2
+    assert p.error_msg == "compressed input is shorter than the format requires"
 
 
 def cases():
@@ -100,3 +127,37 @@ def test_gpu_pointers_off_vector_alignment(cuda):
     out = torch.zeros(n + 3, dtype=torch.int16, device="cuda")
     q = legacy.compress(base[1:1 + n], 0.01, out=out[1:1 + n])
     assert np.array_equal(q.cpu().numpy(), oracle.frsz1_compress(x, 0.01))
+
+
+@pytest.mark.gpu
+def test_gpu_plugin_equals_oracle(cuda):
+    # the plugin front end on host arrays and on device tensors: the same
+    # int16 stream as the oracle (as bytes) and the reference decode
+    p = legacy.Frsz1Plugin()
+    p.set_options({"frsz:epsilon": 5.0})
+    f = np.array([10.0, 20.0, 30.0, 20.0, 10.0], dtype=np.float32)  # test/test_frsz.cc:29-46
+    rc, buf = p.compress(f)
+    assert rc == 0 and buf.dtype == np.uint8 and buf.view(np.int16).tolist() == [1, 1, 1, -1, -1]
+    out = np.zeros(5, dtype=np.float32)
+    assert p.decompress(buf, out) == 0 and np.array_equal(out, f)
+    for dtype, shape, eps in ((np.float32, (70_001,), 1e-3), (np.float64, (3, 1, 4_099), 0.5),
+                              (np.float64, (1, 65_536), 1e-7), (np.float32, (257, 9), 1e-4)):
+        p.set_options({"frsz:epsilon": eps})
+        x = workloads.normal_np(int(np.prod(shape)), dtype, seed=11).reshape(shape) * dtype(10.0)
+        n = legacy.legacy_length(shape)
+        want = oracle.frsz1_compress(np.ascontiguousarray(x).reshape(-1)[:n], eps)
+        yw = oracle.frsz1_decompress(want, dtype, eps)
+        uint = np.uint64 if dtype == np.float64 else np.uint32
+        rc, hbuf = p.compress(x)
+        assert rc == 0 and np.array_equal(hbuf.view(np.int16), want), (dtype, shape)
+        rc, dbuf = p.compress(torch.from_numpy(x).cuda())
+        assert rc == 0 and dbuf.dtype == torch.uint8 and np.array_equal(dbuf.cpu().numpy(), hbuf)
+        host_out = np.full(shape, -1.0, dtype=dtype)
+        assert p.decompress(hbuf, host_out) == 0
+        assert np.array_equal(host_out.reshape(-1)[:n].view(uint), yw.view(uint))
+        assert np.all(host_out.reshape(-1)[n:] == -1.0)
+        dev_out = torch.full(shape, -1.0, dtype=torch.from_numpy(x).dtype, device="cuda")
+        assert p.decompress(dbuf, dev_out) == 0
+        assert np.array_equal(dev_out.cpu().numpy().reshape(-1).view(uint), host_out.reshape(-1).view(uint))
+    p.set_options({"frsz:epsilon": 0.0})
+    assert p.compress(f)[0] == 2 and p.error_code == 2
