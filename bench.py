@@ -457,7 +457,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
         "errors": errors,
         "cpu_baseline": cpu,
         "e2e": e2e,
-        "gpu_launches": 2 * K,
+        "gpu_launches": 3 * K,  # dot: item kernel + final sum; axpy: one kernel
         "clocks": clk,
     }
     print(json.dumps(line), flush=True)
@@ -685,7 +685,7 @@ def run_krylov(args, rank: int, world: int, local_rank: int) -> None:
         "uncompressed_torch": {"dot_ms": round(ms_dense_dot, 4), "axpy_ms": round(ms_dense_axpy, 4)},
         "speedup_fused_dot_vs_uncompressed": round(ms_dense_dot / ms_dot, 2),
         "speedup_fused_axpy_vs_uncompressed": round(ms_dense_axpy / ms_axpy, 2),
-        "gpu_launches": 2 * K,
+        "gpu_launches": 3 * K,  # dot: item kernel + final sum; axpy: one kernel
     }
     print(json.dumps(line), flush=True)
 

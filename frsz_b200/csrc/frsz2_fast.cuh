@@ -883,13 +883,13 @@ __device__ __forceinline__ void fast_load_lane(const std::uint8_t* __restrict__ 
   }
 }
 
+// The P codes of a loaded lane, in value order.
 template<class T, int BITS>
-__device__ __forceinline__ void fast_decode_loaded(const lane_words<T, BITS>& lw, T (&out)[fast_cfg<T, BITS>::P])
+__device__ __forceinline__ void fast_codes_loaded(const lane_words<T, BITS>& lw,
+                                                  typename fast_cfg<T, BITS>::C (&c)[fast_cfg<T, BITS>::P])
 {
   using Cfg = fast_cfg<T, BITS>;
-  using U = typename Cfg::U;
-  using C = typename Cfg::C;
-  constexpr int P = Cfg::P, NW = Cfg::NW;
+  constexpr int NW = Cfg::NW;
   std::uint32_t seg[NW + 1];
   if constexpr (Cfg::ALIGNED) {
 #pragma unroll
@@ -900,8 +900,18 @@ __device__ __forceinline__ void fast_decode_loaded(const lane_words<T, BITS>& lw
     for (int i = 0; i < NW; ++i) seg[i] = __funnelshift_r(lw.w[i], lw.w[i + 1], lw.o);
     seg[NW] = 0;
   }
-  C c[P];
   unpack_all<0, BITS>(seg, c);
+}
+
+template<class T, int BITS>
+__device__ __forceinline__ void fast_decode_loaded(const lane_words<T, BITS>& lw, T (&out)[fast_cfg<T, BITS>::P])
+{
+  using Cfg = fast_cfg<T, BITS>;
+  using U = typename Cfg::U;
+  using C = typename Cfg::C;
+  constexpr int P = Cfg::P;
+  C c[P];
+  fast_codes_loaded<T, BITS>(lw, c);
   const std::int64_t be = lw.be;
   if (plain_exponent<T>(be)) {
     const T inv = pow2<T>((int)be - BITS + 2);

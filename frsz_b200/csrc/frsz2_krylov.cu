@@ -48,6 +48,92 @@ struct BasisGeo
   int log2E;
 };
 
+#ifndef FRSZ2_KRYLOV_NOCVT
+#define FRSZ2_KRYLOV_NOCVT 1
+#endif
+
+// Values of widths up to 32 bits without an integer-to-double conversion,
+// exactly the values fast_decode_loaded gives.  With t = code << (32 - BITS)
+// (sign at bit 31) and m = max(t << 1, 1), a value is m * 2^(be-31): for a
+// nonzero magnitude m = mag * 2^(33-BITS), so m * 2^(be-31) =
+// mag * 2^(be-BITS+2); for a zero magnitude m = 1 gives the decoder's
+// 2^(be-31).  m * 2^(be-31) = D - 2^(be+21) exactly, where D has exponent
+// be+21 and m in the low 32 bits of its mantissa (m < 2^32; the subtraction
+// of two doubles within a factor of 2 is exact).  Needs be+1044 to be a
+// normal exponent field and be in the plain range: be in [-959, 1002].
+// The value's sign goes onto the other factor of the product (sign_onto).
+template<int BITS>
+__device__ __forceinline__ bool nocvt_block(std::int64_t be)
+{
+  return FRSZ2_KRYLOV_NOCVT && BITS <= 32 && be >= -959 && be <= 1002;
+}
+
+__device__ __forceinline__ double nocvt_magnitude(std::uint32_t t, int hi, double base)
+{
+  const std::uint32_t m = max(t << 1, 1u);
+  return __hiloint2double(hi, (int)m) - base;
+}
+
+__device__ __forceinline__ double sign_onto(double x, std::uint32_t t)
+{
+  return __hiloint2double(__double2hiint(x) ^ (int)(t & 0x80000000u), __double2loint(x));
+}
+
+// acc + sum over the lane's values of v[k] * wv[k], FMAs in value order.
+template<int BITS>
+__device__ __forceinline__ double lane_dot(const lane_words<double, BITS>& lw,
+                                           const double (&wv)[fast_cfg<double, BITS>::P], double acc)
+{
+  constexpr int P = fast_cfg<double, BITS>::P;
+  if constexpr (BITS <= 32) {
+    const std::int64_t be = lw.be;
+    if (nocvt_block<BITS>(be)) {
+      std::uint32_t c[P];
+      fast_codes_loaded<double, BITS>(lw, c);
+      const int hi = (int)((std::uint32_t)(be + 1044) << 20);
+      const double base = __hiloint2double(hi, 0);
+#pragma unroll
+      for (int k = 0; k < P; ++k) {
+        const std::uint32_t t = c[k] << (32 - BITS);
+        acc = fma(nocvt_magnitude(t, hi, base), sign_onto(wv[k], t), acc);
+      }
+      return acc;
+    }
+  }
+  double v[P];
+  fast_decode_loaded<double, BITS>(lw, v);
+#pragma unroll
+  for (int k = 0; k < P; ++k) acc = fma(v[k], wv[k], acc);
+  return acc;
+}
+
+// acc[k] + cj * v[k] for the lane's values.
+template<int BITS>
+__device__ __forceinline__ void lane_axpy(const lane_words<double, BITS>& lw, double cj,
+                                          double (&acc)[fast_cfg<double, BITS>::P])
+{
+  constexpr int P = fast_cfg<double, BITS>::P;
+  if constexpr (BITS <= 32) {
+    const std::int64_t be = lw.be;
+    if (nocvt_block<BITS>(be)) {
+      std::uint32_t c[P];
+      fast_codes_loaded<double, BITS>(lw, c);
+      const int hi = (int)((std::uint32_t)(be + 1044) << 20);
+      const double base = __hiloint2double(hi, 0);
+#pragma unroll
+      for (int k = 0; k < P; ++k) {
+        const std::uint32_t t = c[k] << (32 - BITS);
+        acc[k] = fma(sign_onto(cj, t), nocvt_magnitude(t, hi, base), acc[k]);
+      }
+      return;
+    }
+  }
+  double v[P];
+  fast_decode_loaded<double, BITS>(lw, v);
+#pragma unroll
+  for (int k = 0; k < P; ++k) acc[k] = fma(cj, v[k], acc[k]);
+}
+
 template<int BITS>
 __global__ void __launch_bounds__(kKT, kMinCtas)
   k_basis_dot(const __grid_constant__ BasisParams bp, int m, BasisGeo g, const double* __restrict__ w,
@@ -86,12 +172,7 @@ __global__ void __launch_bounds__(kKT, kMinCtas)
         for (int k = 0; k < P; ++k) wv[k] = i + k < len ? s_w[i + k] : 0.0;
 #pragma unroll
         for (int jj = 0; jj < kJB; ++jj)
-          if (j0 + jj < m) {
-            double v[P];
-            fast_decode_loaded<double, BITS>(lw[jj], v);
-#pragma unroll
-            for (int k = 0; k < P; ++k) acc[jj] = fma(v[k], wv[k], acc[jj]);
-          }
+          if (j0 + jj < m) acc[jj] = lane_dot<BITS>(lw[jj], wv, acc[jj]);
       }
 #pragma unroll
       for (int jj = 0; jj < kJB; ++jj) {
@@ -173,12 +254,7 @@ __global__ void __launch_bounds__(kKT, kMinCtas)
         for (int k = 0; k < P; ++k) wv[k] = i + k < len ? s_w[i + k] : 0.0;
 #pragma unroll
         for (int jj = 0; jj < kJB; ++jj)
-          if (j0 + jj < je) {
-            double v[P];
-            fast_decode_loaded<double, BITS>(lw[jj], v);
-#pragma unroll
-            for (int k = 0; k < P; ++k) acc[jj] = fma(v[k], wv[k], acc[jj]);
-          }
+          if (j0 + jj < je) acc[jj] = lane_dot<BITS>(lw[jj], wv, acc[jj]);
       }
 #pragma unroll
       for (int jj = 0; jj < kJB; ++jj) {
@@ -255,13 +331,7 @@ __global__ void __launch_bounds__(kKT, kMinCtas)
         }
 #pragma unroll
       for (int jj = 0; jj < kJB; ++jj)
-        if (j0 + jj < m) {
-          double v[P];
-          fast_decode_loaded<double, BITS>(lw[jj], v);
-          const double cj = s_c[j0 + jj];
-#pragma unroll
-          for (int k = 0; k < P; ++k) acc[k] = fma(cj, v[k], acc[k]);
-        }
+        if (j0 + jj < m) lane_axpy<BITS>(lw[jj], s_c[j0 + jj], acc);
     }
     if (whole) {
       std::uint32_t v[8];
