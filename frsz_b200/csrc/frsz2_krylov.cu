@@ -33,7 +33,16 @@ constexpr int kSub = 3072;          // w values staged per step (24 KiB)
 #ifndef FRSZ2_KRYLOV_MIN_CTAS
 #define FRSZ2_KRYLOV_MIN_CTAS 4
 #endif
-constexpr int kJB = FRSZ2_KRYLOV_JB;             // basis vectors whose loads are in flight together
+// Basis vectors whose loads are in flight together, per kernel and width.
+// Measured on B200 (100 vectors of 2^22 values, 4 CTAs per SM): the dot is
+// fastest with 4 at 32 bits (0.89 of HBM against 0.83 with 6) and with 6 at 16
+// and 24 bits (0.48 against 0.46, 0.68 against 0.66); the axpy with 6 at 16, 24
+// and 32 bits (0.66 against 0.61, 0.87 against 0.82, 1.03 against 1.02).  At
+// 21 bits 6 spills registers and halves the speed; 21, 48 and 64 bits keep
+// FRSZ2_KRYLOV_JB.
+constexpr int kJB = FRSZ2_KRYLOV_JB;
+__host__ __device__ constexpr int jb_dot(int bits) { return bits == 16 || bits == 24 ? 6 : kJB; }
+__host__ __device__ constexpr int jb_axpy(int bits) { return bits == 16 || bits == 24 || bits == 32 ? 6 : kJB; }
 constexpr int kMinCtas = FRSZ2_KRYLOV_MIN_CTAS; // resident CTAs per SM the register budget must allow
 
 struct BasisParams
@@ -141,6 +150,7 @@ __global__ void __launch_bounds__(kKT, kMinCtas)
               double* __restrict__ h)
 {
   constexpr int P = fast_cfg<double, BITS>::P;
+  constexpr int JB = jb_dot(BITS);
   __shared__ double s_w[kSub];
   __shared__ double s_acc[kKT / 32][kMaxBasis];
   __shared__ bool s_last;
@@ -154,15 +164,15 @@ __global__ void __launch_bounds__(kKT, kMinCtas)
     __syncthreads(); // previous slice fully consumed
     for (int i = tid; i < len; i += kKT) s_w[i] = __ldg(w + s0 + i);
     __syncthreads();
-    // kJB vectors at a time: all their loads are issued before any decode
-    for (int j0 = 0; j0 < m; j0 += kJB) {
-      double acc[kJB];
+    // JB vectors at a time: all their loads are issued before any decode
+    for (int j0 = 0; j0 < m; j0 += JB) {
+      double acc[JB];
 #pragma unroll
-      for (int jj = 0; jj < kJB; ++jj) acc[jj] = 0.0;
+      for (int jj = 0; jj < JB; ++jj) acc[jj] = 0.0;
       for (int i = tid * P; i < len; i += kKT * P) {
-        lane_words<double, BITS> lw[kJB];
+        lane_words<double, BITS> lw[JB];
 #pragma unroll
-        for (int jj = 0; jj < kJB; ++jj)
+        for (int jj = 0; jj < JB; ++jj)
           if (j0 + jj < m) {
             const std::uint8_t* buf = bp.buf[j0 + jj];
             fast_load_lane<double, BITS>(buf, buf + g.exp_bytes, g.log2E, s0 + (std::uint64_t)i, lw[jj]);
@@ -171,11 +181,11 @@ __global__ void __launch_bounds__(kKT, kMinCtas)
 #pragma unroll
         for (int k = 0; k < P; ++k) wv[k] = i + k < len ? s_w[i + k] : 0.0;
 #pragma unroll
-        for (int jj = 0; jj < kJB; ++jj)
+        for (int jj = 0; jj < JB; ++jj)
           if (j0 + jj < m) acc[jj] = lane_dot<BITS>(lw[jj], wv, acc[jj]);
       }
 #pragma unroll
-      for (int jj = 0; jj < kJB; ++jj) {
+      for (int jj = 0; jj < JB; ++jj) {
         double a = acc[jj];
 #pragma unroll
         for (int s = 16; s > 0; s >>= 1) a += __shfl_down_sync(0xFFFFFFFFu, a, s);
@@ -217,6 +227,7 @@ __global__ void __launch_bounds__(kKT, kMinCtas)
                   unsigned int ns, int vg, double* __restrict__ partials, unsigned int* __restrict__ next_item)
 {
   constexpr int P = fast_cfg<double, BITS>::P;
+  constexpr int JB = jb_dot(BITS);
   __shared__ double s_w[kSub];
   __shared__ double s_acc[kKT / 32][kMaxBasis];
   __shared__ unsigned int s_item;
@@ -236,15 +247,15 @@ __global__ void __launch_bounds__(kKT, kMinCtas)
     const int len = (int)((g.n - s0) < (std::uint64_t)kSub ? (g.n - s0) : (std::uint64_t)kSub);
     for (int i = tid; i < len; i += kKT) s_w[i] = __ldg(w + s0 + i);
     __syncthreads();
-    // kJB vectors at a time: all their loads are issued before any decode
-    for (int j0 = jb; j0 < je; j0 += kJB) {
-      double acc[kJB];
+    // JB vectors at a time: all their loads are issued before any decode
+    for (int j0 = jb; j0 < je; j0 += JB) {
+      double acc[JB];
 #pragma unroll
-      for (int jj = 0; jj < kJB; ++jj) acc[jj] = 0.0;
+      for (int jj = 0; jj < JB; ++jj) acc[jj] = 0.0;
       for (int i = tid * P; i < len; i += kKT * P) {
-        lane_words<double, BITS> lw[kJB];
+        lane_words<double, BITS> lw[JB];
 #pragma unroll
-        for (int jj = 0; jj < kJB; ++jj)
+        for (int jj = 0; jj < JB; ++jj)
           if (j0 + jj < je) {
             const std::uint8_t* buf = bp.buf[j0 + jj];
             fast_load_lane<double, BITS>(buf, buf + g.exp_bytes, g.log2E, s0 + (std::uint64_t)i, lw[jj]);
@@ -253,11 +264,11 @@ __global__ void __launch_bounds__(kKT, kMinCtas)
 #pragma unroll
         for (int k = 0; k < P; ++k) wv[k] = i + k < len ? s_w[i + k] : 0.0;
 #pragma unroll
-        for (int jj = 0; jj < kJB; ++jj)
+        for (int jj = 0; jj < JB; ++jj)
           if (j0 + jj < je) acc[jj] = lane_dot<BITS>(lw[jj], wv, acc[jj]);
       }
 #pragma unroll
-      for (int jj = 0; jj < kJB; ++jj) {
+      for (int jj = 0; jj < JB; ++jj) {
         double a = acc[jj];
 #pragma unroll
         for (int sh = 16; sh > 0; sh >>= 1) a += __shfl_down_sync(0xFFFFFFFFu, a, sh);
@@ -305,6 +316,7 @@ __global__ void __launch_bounds__(kKT, kMinCtas)
                double* __restrict__ y)
 {
   constexpr int P = fast_cfg<double, BITS>::P;
+  constexpr int JB = jb_axpy(BITS);
   __shared__ double s_c[kMaxBasis];
   for (int j = threadIdx.x; j < m; j += kKT) s_c[j] = __ldg(coef + j);
   __syncthreads();
@@ -321,16 +333,16 @@ __global__ void __launch_bounds__(kKT, kMinCtas)
 #pragma unroll
       for (int k = 0; k < P; ++k) acc[k] = idx + k < g.n ? y[idx + k] : 0.0;
     }
-    for (int j0 = 0; j0 < m; j0 += kJB) {
-      lane_words<double, BITS> lw[kJB];
+    for (int j0 = 0; j0 < m; j0 += JB) {
+      lane_words<double, BITS> lw[JB];
 #pragma unroll
-      for (int jj = 0; jj < kJB; ++jj)
+      for (int jj = 0; jj < JB; ++jj)
         if (j0 + jj < m) {
           const std::uint8_t* buf = bp.buf[j0 + jj];
           fast_load_lane<double, BITS>(buf, buf + g.exp_bytes, g.log2E, idx, lw[jj]);
         }
 #pragma unroll
-      for (int jj = 0; jj < kJB; ++jj)
+      for (int jj = 0; jj < JB; ++jj)
         if (j0 + jj < m) lane_axpy<BITS>(lw[jj], s_c[j0 + jj], acc);
     }
     if (whole) {
@@ -467,7 +479,7 @@ int frsz2_basis_dot(int dtype, int bits, int block_size, const void* const* basi
     }
     const std::uint64_t ctas = (std::uint64_t)sm_count() * (std::uint64_t)per;
     // vectors per item: up to 32 vectors, all of them (whole slices); more,
-    // about 8 items per CTA in multiples of kJB and at least 16 vectors (each
+    // about 8 items per CTA in multiples of jb_dot and at least 16 vectors (each
     // item stages its slice of w once).  Measured on B200 with 2^22-value
     // vectors, 32 bits: m = 100 0.76 of HBM with 32 vectors per item against
     // 0.74 with whole slices; m = 20 0.67 with whole slices against 0.62 with
@@ -475,7 +487,8 @@ int frsz2_basis_dot(int dtype, int bits, int block_size, const void* const* basi
     std::uint64_t vg = (std::uint64_t)m;
     if (m > 32) {
       vg = ((std::uint64_t)m * ns + 8 * ctas - 1) / (8 * ctas);
-      vg = std::min<std::uint64_t>((std::uint64_t)m, std::max<std::uint64_t>(16, (vg + kJB - 1) / kJB * kJB));
+      const std::uint64_t jb = (std::uint64_t)jb_dot(bits);
+      vg = std::min<std::uint64_t>((std::uint64_t)m, std::max<std::uint64_t>(16, (vg + jb - 1) / jb * jb));
     }
     const std::uint64_t items = ns * (((std::uint64_t)m + vg - 1) / vg);
     if (items > 0xFFFFFFFFull) return set_error(FRSZ2_EFAIL, "basis vectors too long");
