@@ -1,0 +1,267 @@
+// frsz2_blockwise.cuh -- compile-time-width kernels for exponent blocks of
+// up to kBwMaxE values of any size (such as the reference tests' 5): one
+// thread per exponent block.
+//
+// A CTA takes a chunk of bw_threads * bpt whole blocks.  Compress: the chunk's
+// values come into shared memory with 16-byte loads; each thread reads its
+// block's values (at most kBwMaxE, unrolled, so every code lands at a
+// compile-time bit position), takes the block exponent, encodes and packs
+// the codes into W-bit words in registers and writes them to a second
+// shared-memory region, the chunk's block image, which leaves with 16-byte
+// stores; the exponents leave with one store per thread.  Decompress runs
+// the other way.  The per-value arithmetic is the fast kernels' (float
+// scaling in the plain exponent range, the exact integer restatement
+// elsewhere), so the bytes and values are the reference's bit for bit.
+//
+// Needs values aligned to the element size and the compressed buffer to the
+// word size (the C ABI checks both); any E from 1 to kBwMaxE.
+#pragma once
+
+#include "frsz2_chunked.cuh"
+
+#include <algorithm>
+#include <array>
+#include <utility>
+
+namespace frsz2b {
+
+constexpr int kBwMaxE = 16;       // largest block size
+constexpr int kBwBytes = 16384;   // bytes of values per chunk aimed at
+constexpr int kBwMaxBpt = 4;      // blocks per thread per chunk at most
+
+// Threads per CTA: 256 for fp32, 128 for fp64, so that a chunk's two regions
+// stay within the default 48 KB of dynamic shared memory for every E.
+template<class T>
+constexpr int bw_threads()
+{
+  return sizeof(T) == 4 ? 256 : 128;
+}
+
+template<int W>
+using bw_word_t = std::conditional_t<
+  (W == 8), std::uint8_t,
+  std::conditional_t<(W == 16), std::uint16_t, std::conditional_t<(W == 32), std::uint32_t, std::uint64_t>>>;
+
+// Blocks per thread per chunk for block size E.
+template<class T>
+__host__ __device__ inline int bw_bpt(int E)
+{
+  const int b = kBwBytes / (bw_threads<T>() * E * (int)sizeof(T));
+  return b < 1 ? 1 : (b > kBwMaxBpt ? kBwMaxBpt : b);
+}
+
+// Bytes of the values region (the block image region has the same size: a
+// block's bytes never exceed its values' bytes, since W divides the float
+// width).  Each region carries 16 bytes for the alignment offset.
+template<class T>
+__host__ __device__ inline std::uint32_t bw_region_bytes(int E)
+{
+  return (std::uint32_t)(bw_threads<T>() * bw_bpt<T>(E) * E) * (std::uint32_t)sizeof(T) + 16u;
+}
+template<class T>
+__host__ __device__ inline std::size_t bw_smem_bytes(int E)
+{
+  return 2 * (std::size_t)bw_region_bytes<T>(E);
+}
+// The most any block size up to kBwMaxE needs: 32,800 bytes for both types.
+template<class T>
+constexpr std::size_t bw_smem_max()
+{
+  return 2 * ((std::size_t)bw_threads<T>() * kBwMaxE * sizeof(T) + 16);
+}
+static_assert(bw_smem_max<float>() <= 48 * 1024 && bw_smem_max<double>() <= 48 * 1024, "default shared memory");
+
+template<class T, int BITS>
+__global__ void __launch_bounds__(bw_threads<T>()) k_compress_blockwise(Job j)
+{
+  using Cfg = fast_cfg<T, BITS>;
+  using U = typename Cfg::U;
+  using C = typename Cfg::C;
+  using K = key_of<T>;
+  constexpr int W = Cfg::W;
+  using Word = bw_word_t<W>;
+  constexpr int NWMAX = (kBwMaxE * BITS + W - 1) / W;
+  extern __shared__ __align__(16) std::uint8_t s_chunk[];
+
+  const T* __restrict__ x = static_cast<const T*>(j.values_in);
+  const int tid = threadIdx.x;
+  const int E = j.E;
+  const std::uint32_t BB = j.block_bytes;
+  const int bpt = bw_bpt<T>(E);
+  constexpr int NT = bw_threads<T>();
+  const int nbc = NT * bpt;
+  std::uint8_t* s_val = s_chunk;
+  std::uint8_t* s_img = s_chunk + bw_region_bytes<T>(E);
+  const std::uint64_t nb = (j.n + (std::uint64_t)E - 1) / (std::uint64_t)E;
+  const std::uint64_t nchunks = (nb + (std::uint64_t)nbc - 1) / (std::uint64_t)nbc;
+
+  for (std::uint64_t ch = blockIdx.x; ch < nchunks; ch += gridDim.x) {
+    const std::uint64_t b0 = ch * (std::uint64_t)nbc;
+    const std::uint64_t v0 = b0 * (std::uint64_t)E;
+    const int nv = (int)(j.n - v0 < (std::uint64_t)(nbc * E) ? j.n - v0 : (std::uint64_t)(nbc * E));
+    const int nbk = (nv + E - 1) / E;
+    const std::uint8_t* gin = reinterpret_cast<const std::uint8_t*>(x + v0);
+    std::uint8_t* gout = j.words + b0 * (std::uint64_t)BB;
+    const std::uint32_t hv = (std::uint32_t)(reinterpret_cast<std::uintptr_t>(gin) & 15u);
+    const std::uint32_t hw = (std::uint32_t)(reinterpret_cast<std::uintptr_t>(gout) & 15u);
+    chunk_copy<false>(const_cast<std::uint8_t*>(gin), s_val, (std::uint32_t)nv * (std::uint32_t)sizeof(T));
+    __syncthreads();
+
+    for (int b = tid; b < nbk; b += NT) {
+      const T* sv = reinterpret_cast<const T*>(s_val + hv) + b * E;
+      const int cnt = min(E, nv - b * E);
+      // Loops run to the block's count: fully unrolled (registers and bit
+      // positions stay compile-time) with a branch out after value cnt - 1,
+      // uniform across the warp except in the array's last block.
+      U u[kBwMaxE];
+      std::uint32_t kr = 0;
+#pragma unroll
+      for (int k = 0; k < kBwMaxE; ++k) {
+        if (k >= cnt) break;
+        u[k] = to_bits<T>(sv[k]);
+        kr = max(kr, K::raw(u[k]));
+      }
+      // block exponent: the largest non-NaN magnitude's (std::max semantics)
+      std::uint32_t kc = kr;
+      if (kr >= K::SPECIAL) {
+        kc = 0;
+#pragma unroll
+        for (int k = 0; k < kBwMaxE; ++k) {
+          if (k >= cnt) break;
+          kc = max(kc, K::clean(u[k]));
+        }
+      }
+      const std::int64_t ex = exponent_of_field<T>((int)(kc >> K::FSHIFT));
+      const std::int64_t be = wrap_signed(ex, W);
+      const bool plain = kr < K::SPECIAL && be == ex && plain_exponent<T>(be);
+      const T scale = pow2<T>(plain ? BITS - 2 - (int)be : 0);
+      Word acc[NWMAX];
+#pragma unroll
+      for (int w = 0; w < NWMAX; ++w) acc[w] = 0;
+#pragma unroll
+      for (int k = 0; k < kBwMaxE; ++k) {
+        if (k >= cnt) break;
+        const C c = plain ? encode_plain<T, BITS>(u[k], scale) : (C)to_code<T>(u[k], (std::int16_t)be, BITS);
+        const int p = k * BITS, w = p / W, o = p % W; // compile-time after unrolling
+        acc[w] |= (Word)(c << o);
+        if (o + BITS > W) acc[w + 1] |= (Word)(c >> (W - o));
+      }
+      // only the words the block's values reach (the array's last block)
+      const int nw = (int)(written_block_bytes(cnt, BITS, W) / (W / 8));
+      Word* dst = reinterpret_cast<Word*>(s_img + hw + (std::uint32_t)b * BB);
+#pragma unroll
+      for (int w = 0; w < NWMAX; ++w) {
+        if (w >= nw) break;
+        dst[w] = acc[w];
+      }
+      store_word(j.exps + (b0 + (std::uint64_t)b) * (std::uint64_t)(W / 8), (std::uint64_t)be, W);
+    }
+    __syncthreads();
+    const int last_cnt = nv - (nbk - 1) * E;
+    const std::uint32_t out_bytes = (std::uint32_t)(nbk - 1) * BB + written_block_bytes(last_cnt, BITS, W);
+    chunk_copy<true>(gout, s_img, out_bytes);
+    __syncthreads(); // shared memory is reused by the next chunk
+  }
+}
+
+template<class T, int BITS>
+__global__ void __launch_bounds__(bw_threads<T>()) k_decompress_blockwise(Job j)
+{
+  using Cfg = fast_cfg<T, BITS>;
+  using U = typename Cfg::U;
+  using C = typename Cfg::C;
+  constexpr int W = Cfg::W;
+  using Word = bw_word_t<W>;
+  constexpr int NWMAX = (kBwMaxE * BITS + W - 1) / W;
+  constexpr int CBITS = 8 * (int)sizeof(C);
+  constexpr C CMASK = BITS == CBITS ? ~C(0) : (C)((C(1) << (BITS % CBITS)) - C(1));
+  extern __shared__ __align__(16) std::uint8_t s_chunk[];
+
+  T* __restrict__ y = static_cast<T*>(j.values_out);
+  const int tid = threadIdx.x;
+  const int E = j.E;
+  const std::uint32_t BB = j.block_bytes;
+  const int nwb = (int)(BB / (W / 8));
+  const int bpt = bw_bpt<T>(E);
+  constexpr int NT = bw_threads<T>();
+  const int nbc = NT * bpt;
+  std::uint8_t* s_val = s_chunk;
+  std::uint8_t* s_img = s_chunk + bw_region_bytes<T>(E);
+  const std::uint64_t nb = (j.n + (std::uint64_t)E - 1) / (std::uint64_t)E;
+  const std::uint64_t nchunks = (nb + (std::uint64_t)nbc - 1) / (std::uint64_t)nbc;
+
+  for (std::uint64_t ch = blockIdx.x; ch < nchunks; ch += gridDim.x) {
+    const std::uint64_t b0 = ch * (std::uint64_t)nbc;
+    const std::uint64_t v0 = b0 * (std::uint64_t)E;
+    const int nv = (int)(j.n - v0 < (std::uint64_t)(nbc * E) ? j.n - v0 : (std::uint64_t)(nbc * E));
+    const int nbk = (nv + E - 1) / E;
+    const std::uint8_t* gin = j.words + b0 * (std::uint64_t)BB;
+    std::uint8_t* gout = reinterpret_cast<std::uint8_t*>(y + v0);
+    const std::uint32_t hw = (std::uint32_t)(reinterpret_cast<std::uintptr_t>(gin) & 15u);
+    const std::uint32_t hv = (std::uint32_t)(reinterpret_cast<std::uintptr_t>(gout) & 15u);
+    // whole blocks: the buffer holds every block in full
+    chunk_copy<false>(const_cast<std::uint8_t*>(gin), s_img, (std::uint32_t)nbk * BB);
+    __syncthreads();
+
+    for (int b = tid; b < nbk; b += NT) {
+      const std::int64_t e = load_exp(j.exps + (b0 + (std::uint64_t)b) * (std::uint64_t)(W / 8), W);
+      const Word* src = reinterpret_cast<const Word*>(s_img + hw + (std::uint32_t)b * BB);
+      Word wd[NWMAX];
+#pragma unroll
+      for (int w = 0; w < NWMAX; ++w) {
+        if (w >= nwb) break;
+        wd[w] = src[w];
+      }
+      const int cnt = min(E, nv - b * E);
+      T* sv = reinterpret_cast<T*>(s_val + hv) + b * E;
+      const bool plain = plain_exponent<T>(e);
+      const T inv = pow2<T>(plain ? (int)e - BITS + 2 : 0);
+      const U zero_bits = sizeof(T) == 4 ? (U)((std::uint32_t)(e + 96) << 23) : (U)((std::uint64_t)(e + 992) << 52);
+#pragma unroll
+      for (int k = 0; k < kBwMaxE; ++k) {
+        if (k >= cnt) break;
+        const int p = k * BITS, w = p / W, o = p % W; // compile-time after unrolling
+        C c = (C)((C)wd[w] >> o);
+        if (o + BITS > W) c |= (C)((C)wd[w + 1] << (W - o));
+        c &= CMASK;
+        const U r = plain ? decode_plain<T, BITS>(c, inv, zero_bits) : to_bits<T>(from_code<T>((U)c, e, BITS));
+        sv[k] = from_bits<T>(r);
+      }
+    }
+    __syncthreads();
+    chunk_copy<true>(gout, s_val, (std::uint32_t)nv * (std::uint32_t)sizeof(T));
+    __syncthreads(); // shared memory is reused by the next chunk
+  }
+}
+
+// Launch of one width: one CTA per chunk (the loop covers any grid).
+template<class T, int BITS>
+cudaError_t launch_blockwise_one(bool compress, const Job& j, cudaStream_t s)
+{
+  const std::uint64_t nb = (j.n + (std::uint64_t)j.E - 1) / (std::uint64_t)j.E;
+  const std::uint64_t nbc = (std::uint64_t)bw_threads<T>() * (std::uint64_t)bw_bpt<T>(j.E);
+  const unsigned grid = (unsigned)std::max<std::uint64_t>(1, std::min<std::uint64_t>((nb + nbc - 1) / nbc, 1u << 30));
+  const std::size_t smem = bw_smem_bytes<T>(j.E);
+  if (compress)
+    k_compress_blockwise<T, BITS><<<grid, bw_threads<T>(), smem, s>>>(j);
+  else
+    k_decompress_blockwise<T, BITS><<<grid, bw_threads<T>(), smem, s>>>(j);
+  return cudaGetLastError();
+}
+
+using blockwise_fn = cudaError_t (*)(bool, const Job&, cudaStream_t);
+
+template<class T, int LO, int... I>
+constexpr auto make_blockwise_table(std::integer_sequence<int, I...>)
+{
+  return std::array<blockwise_fn, sizeof...(I)>{ &launch_blockwise_one<T, LO + I>... };
+}
+
+// Whether the blockwise kernels take a job: block sizes up to kBwMaxE (the
+// C ABI has already checked the pointers' alignment).
+inline bool blockwise_eligible(const Job& j) { return j.E >= 1 && j.E <= kBwMaxE; }
+
+cudaError_t launch_blockwise_f32(int bits, bool compress, const Job& j, cudaStream_t s);
+cudaError_t launch_blockwise_f64(int bits, bool compress, const Job& j, cudaStream_t s);
+
+} // namespace frsz2b

@@ -1,5 +1,6 @@
 // frsz2_capi.cu -- C ABI of libfrsz2_b200.so: argument checks, kernel choice,
 // launch geometry, and the host-buffer path with pipelined copies.
+#include "frsz2_blockwise.cuh"
 #include "frsz2_chunked.cuh"
 #include "frsz2_fast_dispatch.hpp"
 #include "frsz2_kernels.cuh"
@@ -158,6 +159,10 @@ static int launch_compress_t(const Job& j, int dtype, cudaStream_t s, bool* used
       k_compress_tile<T, std::uint64_t><<<grid, kNT, compress_smem<T>(j.bits), s>>>(j);
     else
       k_compress_tile<T, std::uint32_t><<<grid, kNT, compress_smem<T>(j.bits), s>>>(j);
+  } else if (blockwise_eligible(j)) {
+    return cuda_status(sizeof(T) == 8 ? launch_blockwise_f64(j.bits, true, j, s)
+                                      : launch_blockwise_f32(j.bits, true, j, s),
+                       "compress launch");
   } else if (j.E <= kChunkMaxECompress) {
     if (j.bits <= 32)
       k_compress_chunked<T, std::uint32_t><<<chunk_grid(j), kNT, 0, s>>>(j);
@@ -187,6 +192,10 @@ static int launch_decompress_t(const Job& j, int dtype, cudaStream_t s, bool* us
       k_decompress_tile<T, std::uint64_t><<<grid, kNT, decompress_smem<T>(j), s>>>(j);
     else
       k_decompress_tile<T, std::uint32_t><<<grid, kNT, decompress_smem<T>(j), s>>>(j);
+  } else if (blockwise_eligible(j)) {
+    return cuda_status(sizeof(T) == 8 ? launch_blockwise_f64(j.bits, false, j, s)
+                                      : launch_blockwise_f32(j.bits, false, j, s),
+                       "decompress launch");
   } else if (j.E <= kChunkMaxEDecompress) {
     if (j.bits <= 32)
       k_decompress_chunked<T, std::uint32_t><<<chunk_grid(j), kNT, 0, s>>>(j);

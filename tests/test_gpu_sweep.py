@@ -111,13 +111,40 @@ def test_nan_inf(cuda, dtype):
 
 @pytest.mark.parametrize("E", [3, 5, 6, 7, 12, 48, 100, 257, 1000, 2047])
 def test_block_sizes_not_powers_of_two(cuda, E):
-    """Block sizes the fast kernels do not take (chunked kernels): several
-    chunks, a partial last block, special values."""
+    """Block sizes the fast kernels do not take (one-thread-per-block kernels
+    up to 16, chunked and warp-per-block kernels above): several chunks, a
+    partial last block, special values."""
     for dtype, widths in ((np.float32, (4, 9, 16, 21, 32)), (np.float64, (5, 8, 21, 33, 52, 64))):
         n = 3 * 2048 + 2 * E + E // 2 + 1
         x = special_values(dtype, n, E)
         for bits in widths:
             check(x, bits, E)
+
+
+@pytest.mark.parametrize("dtype,bits", [(np.float32, b) for b in range(4, 33)] + [(np.float64, b) for b in range(4, 65)])
+def test_small_blocks_every_width(cuda, dtype, bits):
+    """The one-thread-per-block kernels (block sizes up to 16 that the fast
+    kernels do not take): every width, block sizes 3, 5, 11 and 16 (16 with
+    the values off the 32-byte layout), several chunks of whole blocks, a
+    partial last block, special values."""
+    es = np.dtype(dtype).itemsize
+    for E in (3, 5, 11, 16):
+        n = (5 * 4096 if es == 4 else 5 * 2048) + 2 * E + E // 2 + 1
+        x = special_values(dtype, n, bits * 31 + E)
+        if E != 16:
+            check(x, bits, E)
+            continue
+        tv = torch.zeros(n + 1, dtype=torch.float32 if es == 4 else torch.float64, device="cuda")
+        tv[1:] = torch.from_numpy(x).cuda()
+        size = frsz_b200.compressed_size(dtype, bits, E, n)
+        buf = torch.full((size,), 0x33, dtype=torch.uint8, device="cuda")
+        frsz_b200.compress(tv[1:], bits, E, out=buf)
+        ref = oracle.compress(x, bits, E, canary=0x33)
+        assert np.array_equal(buf.cpu().numpy(), ref), (bits, E)
+        out = torch.zeros(n + 1, dtype=tv.dtype, device="cuda")
+        frsz_b200.decompress(torch.from_numpy(ref).cuda(), n, dtype, bits, E, out=out[1:])
+        uint = np.uint64 if es == 8 else np.uint32
+        assert np.array_equal(out[1:].cpu().numpy().view(uint), oracle.decompress(ref, n, dtype, bits, E).view(uint))
 
 
 @pytest.mark.parametrize("dtype,bits,E", [(np.float32, 16, 32), (np.float32, 21, 8), (np.float64, 40, 4),
