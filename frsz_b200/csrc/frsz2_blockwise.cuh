@@ -18,6 +18,7 @@
 #pragma once
 
 #include "frsz2_chunked.cuh"
+#include "frsz2_launch.hpp"
 
 #include <algorithm>
 #include <array>
@@ -25,9 +26,30 @@
 
 namespace frsz2b {
 
+#ifndef FRSZ2_BW_BYTES_F32
+#define FRSZ2_BW_BYTES_F32 16384
+#endif
+#ifndef FRSZ2_BW_PIPE_F32
+#define FRSZ2_BW_PIPE_F32 1
+#endif
+#ifndef FRSZ2_BW_PIPE_F64
+#define FRSZ2_BW_PIPE_F64 1
+#endif
 constexpr int kBwMaxE = 16;       // largest block size
-constexpr int kBwBytes = 16384;   // bytes of values per chunk aimed at
 constexpr int kBwMaxBpt = 4;      // blocks per thread per chunk at most
+
+// Bytes of values per chunk aimed at.
+template<class T>
+constexpr int bw_bytes()
+{
+  return sizeof(T) == 4 ? FRSZ2_BW_BYTES_F32 : 16384;
+}
+// Whether a CTA loads the next chunk while it works on the current one.
+template<class T>
+constexpr bool bw_pipe()
+{
+  return sizeof(T) == 4 ? FRSZ2_BW_PIPE_F32 != 0 : FRSZ2_BW_PIPE_F64 != 0;
+}
 
 // Threads per CTA: 256 for fp32, 128 for fp64, so that a chunk's two regions
 // stay within the default 48 KB of dynamic shared memory for every E.
@@ -35,6 +57,19 @@ template<class T>
 constexpr int bw_threads()
 {
   return sizeof(T) == 4 ? 256 : 128;
+}
+
+#ifndef FRSZ2_BW_MIN_CTAS_F32
+#define FRSZ2_BW_MIN_CTAS_F32 1
+#endif
+#ifndef FRSZ2_BW_MIN_CTAS_F64
+#define FRSZ2_BW_MIN_CTAS_F64 1
+#endif
+// Resident CTAs per SM the register budget must allow.
+template<class T>
+constexpr int bw_min_ctas()
+{
+  return sizeof(T) == 4 ? FRSZ2_BW_MIN_CTAS_F32 : FRSZ2_BW_MIN_CTAS_F64;
 }
 
 template<int W>
@@ -46,7 +81,7 @@ using bw_word_t = std::conditional_t<
 template<class T>
 __host__ __device__ inline int bw_bpt(int E)
 {
-  const int b = kBwBytes / (bw_threads<T>() * E * (int)sizeof(T));
+  const int b = bw_bytes<T>() / (bw_threads<T>() * E * (int)sizeof(T));
   return b < 1 ? 1 : (b > kBwMaxBpt ? kBwMaxBpt : b);
 }
 
@@ -71,8 +106,62 @@ constexpr std::size_t bw_smem_max()
 }
 static_assert(bw_smem_max<float>() <= 48 * 1024 && bw_smem_max<double>() <= 48 * 1024, "default shared memory");
 
+// Largest chunk of values or block images in bytes, and the 16-byte loads a
+// thread makes of one.
+template<class T>
+constexpr std::uint32_t bw_max_chunk_bytes()
+{
+  return (std::uint32_t)bw_threads<T>() * kBwMaxE * (std::uint32_t)sizeof(T) > (std::uint32_t)bw_bytes<T>()
+           ? (std::uint32_t)bw_threads<T>() * kBwMaxE * (std::uint32_t)sizeof(T)
+           : (std::uint32_t)bw_bytes<T>();
+}
+template<class T>
+constexpr int bw_loads_per_thread()
+{
+  return (int)((bw_max_chunk_bytes<T>() / 16 + bw_threads<T>() - 1) / bw_threads<T>());
+}
+
+// Global -> shared copy of `bytes` (at most bw_max_chunk_bytes) from g to
+// s + (g mod 16), as chunk_copy<false> does, in two steps: bw_issue starts a
+// thread's 16-byte loads into registers, bw_commit stores them (and the odd
+// bytes before g's first and after its last 16-byte boundary).  Issuing the
+// next chunk's loads before working on the current one hides their latency.
+template<int NT, int MAXI>
+__device__ __forceinline__ void bw_issue(const std::uint8_t* g, std::uint32_t bytes, uint4 (&r)[MAXI])
+{
+  const std::uint32_t h = (std::uint32_t)(reinterpret_cast<std::uintptr_t>(g) & 15u);
+  const std::uint32_t head = h == 0 ? 0u : min(16u - h, bytes);
+  const std::uint32_t n16 = (bytes - head) >> 4;
+  const uint4* g16 = reinterpret_cast<const uint4*>(g + head);
+#pragma unroll
+  for (int i = 0; i < MAXI; ++i) {
+    const std::uint32_t k = threadIdx.x + (std::uint32_t)(i * NT);
+    if (k < n16) r[i] = __ldg(g16 + k);
+  }
+}
+
+template<int NT, int MAXI>
+__device__ __forceinline__ void bw_commit(const std::uint8_t* g, std::uint8_t* s, std::uint32_t bytes,
+                                          const uint4 (&r)[MAXI])
+{
+  const std::uint32_t tid = threadIdx.x;
+  const std::uint32_t h = (std::uint32_t)(reinterpret_cast<std::uintptr_t>(g) & 15u);
+  const std::uint32_t head = h == 0 ? 0u : min(16u - h, bytes);
+  const std::uint32_t n16 = (bytes - head) >> 4;
+  const std::uint32_t tail0 = head + (n16 << 4);
+  std::uint8_t* sb = s + h;
+  uint4* s16 = reinterpret_cast<uint4*>(sb + head);
+#pragma unroll
+  for (int i = 0; i < MAXI; ++i) {
+    const std::uint32_t k = tid + (std::uint32_t)(i * NT);
+    if (k < n16) s16[k] = r[i];
+  }
+  if (tid < head) sb[tid] = __ldg(g + tid);
+  for (std::uint32_t i = tail0 + tid; i < bytes; i += NT) sb[i] = __ldg(g + i);
+}
+
 template<class T, int BITS>
-__global__ void __launch_bounds__(bw_threads<T>()) k_compress_blockwise(Job j)
+__global__ void __launch_bounds__(bw_threads<T>(), bw_min_ctas<T>()) k_compress_blockwise(Job j)
 {
   using Cfg = fast_cfg<T, BITS>;
   using U = typename Cfg::U;
@@ -95,18 +184,36 @@ __global__ void __launch_bounds__(bw_threads<T>()) k_compress_blockwise(Job j)
   const std::uint64_t nb = (j.n + (std::uint64_t)E - 1) / (std::uint64_t)E;
   const std::uint64_t nchunks = (nb + (std::uint64_t)nbc - 1) / (std::uint64_t)nbc;
 
-  for (std::uint64_t ch = blockIdx.x; ch < nchunks; ch += gridDim.x) {
+  constexpr int MAXI = bw_loads_per_thread<T>();
+  // chunk ch: its first block, values and the global addresses of both sides
+  auto values_of = [&](std::uint64_t ch, int& nv) {
+    const std::uint64_t v0 = ch * (std::uint64_t)nbc * (std::uint64_t)E;
+    nv = (int)(j.n - v0 < (std::uint64_t)(nbc * E) ? j.n - v0 : (std::uint64_t)(nbc * E));
+    return reinterpret_cast<const std::uint8_t*>(x + v0);
+  };
+  uint4 r[MAXI];
+  std::uint64_t ch = blockIdx.x;
+  if (bw_pipe<T>() && ch < nchunks) {
+    int nv0;
+    const std::uint8_t* g0 = values_of(ch, nv0);
+    bw_issue<NT, MAXI>(g0, (std::uint32_t)nv0 * (std::uint32_t)sizeof(T), r);
+  }
+  for (; ch < nchunks; ch += gridDim.x) {
     const std::uint64_t b0 = ch * (std::uint64_t)nbc;
-    const std::uint64_t v0 = b0 * (std::uint64_t)E;
-    const int nv = (int)(j.n - v0 < (std::uint64_t)(nbc * E) ? j.n - v0 : (std::uint64_t)(nbc * E));
+    int nv;
+    const std::uint8_t* gin = values_of(ch, nv);
+    if (!bw_pipe<T>()) bw_issue<NT, MAXI>(gin, (std::uint32_t)nv * (std::uint32_t)sizeof(T), r);
     const int nbk = (nv + E - 1) / E;
-    const std::uint8_t* gin = reinterpret_cast<const std::uint8_t*>(x + v0);
     std::uint8_t* gout = j.words + b0 * (std::uint64_t)BB;
     const std::uint32_t hv = (std::uint32_t)(reinterpret_cast<std::uintptr_t>(gin) & 15u);
     const std::uint32_t hw = (std::uint32_t)(reinterpret_cast<std::uintptr_t>(gout) & 15u);
-    chunk_copy<false>(const_cast<std::uint8_t*>(gin), s_val, (std::uint32_t)nv * (std::uint32_t)sizeof(T));
+    bw_commit<NT, MAXI>(gin, s_val, (std::uint32_t)nv * (std::uint32_t)sizeof(T), r);
     __syncthreads();
-
+    if (bw_pipe<T>() && ch + gridDim.x < nchunks) { // the next chunk's loads fly while this one is coded
+      int nvn;
+      const std::uint8_t* gn = values_of(ch + gridDim.x, nvn);
+      bw_issue<NT, MAXI>(gn, (std::uint32_t)nvn * (std::uint32_t)sizeof(T), r);
+    }
     for (int b = tid; b < nbk; b += NT) {
       const T* sv = reinterpret_cast<const T*>(s_val + hv) + b * E;
       const int cnt = min(E, nv - b * E);
@@ -138,14 +245,21 @@ __global__ void __launch_bounds__(bw_threads<T>()) k_compress_blockwise(Job j)
       Word acc[NWMAX];
 #pragma unroll
       for (int w = 0; w < NWMAX; ++w) acc[w] = 0;
+      // one loop per arithmetic, so only the block's own runs
+      auto pack = [&](auto encode) {
 #pragma unroll
-      for (int k = 0; k < kBwMaxE; ++k) {
-        if (k >= cnt) break;
-        const C c = plain ? encode_plain<T, BITS>(u[k], scale) : (C)to_code<T>(u[k], (std::int16_t)be, BITS);
-        const int p = k * BITS, w = p / W, o = p % W; // compile-time after unrolling
-        acc[w] |= (Word)(c << o);
-        if (o + BITS > W) acc[w + 1] |= (Word)(c >> (W - o));
-      }
+        for (int k = 0; k < kBwMaxE; ++k) {
+          if (k >= cnt) break;
+          const C c = encode(u[k]);
+          const int p = k * BITS, w = p / W, o = p % W; // compile-time after unrolling
+          acc[w] |= (Word)(c << o);
+          if (o + BITS > W) acc[w + 1] |= (Word)(c >> (W - o));
+        }
+      };
+      if (plain)
+        pack([&](U v) { return encode_plain<T, BITS>(v, scale); });
+      else
+        pack([&](U v) { return (C)to_code<T>(v, (std::int16_t)be, BITS); });
       // only the words the block's values reach (the array's last block)
       const int nw = (int)(written_block_bytes(cnt, BITS, W) / (W / 8));
       Word* dst = reinterpret_cast<Word*>(s_img + hw + (std::uint32_t)b * BB);
@@ -160,12 +274,13 @@ __global__ void __launch_bounds__(bw_threads<T>()) k_compress_blockwise(Job j)
     const int last_cnt = nv - (nbk - 1) * E;
     const std::uint32_t out_bytes = (std::uint32_t)(nbk - 1) * BB + written_block_bytes(last_cnt, BITS, W);
     chunk_copy<true>(gout, s_img, out_bytes);
-    __syncthreads(); // shared memory is reused by the next chunk
+    // no barrier here: the next chunk's commit writes the values region,
+    // which every thread finished reading before the barrier above
   }
 }
 
 template<class T, int BITS>
-__global__ void __launch_bounds__(bw_threads<T>()) k_decompress_blockwise(Job j)
+__global__ void __launch_bounds__(bw_threads<T>(), bw_min_ctas<T>()) k_decompress_blockwise(Job j)
 {
   using Cfg = fast_cfg<T, BITS>;
   using U = typename Cfg::U;
@@ -190,21 +305,51 @@ __global__ void __launch_bounds__(bw_threads<T>()) k_decompress_blockwise(Job j)
   const std::uint64_t nb = (j.n + (std::uint64_t)E - 1) / (std::uint64_t)E;
   const std::uint64_t nchunks = (nb + (std::uint64_t)nbc - 1) / (std::uint64_t)nbc;
 
-  for (std::uint64_t ch = blockIdx.x; ch < nchunks; ch += gridDim.x) {
+  constexpr int MAXI = bw_loads_per_thread<T>();
+  // chunk ch's blocks and values, and the loads of its block image and
+  // exponents
+  auto blocks_of = [&](std::uint64_t ch, int& nv, int& nbk) {
     const std::uint64_t b0 = ch * (std::uint64_t)nbc;
     const std::uint64_t v0 = b0 * (std::uint64_t)E;
-    const int nv = (int)(j.n - v0 < (std::uint64_t)(nbc * E) ? j.n - v0 : (std::uint64_t)(nbc * E));
-    const int nbk = (nv + E - 1) / E;
+    nv = (int)(j.n - v0 < (std::uint64_t)(nbc * E) ? j.n - v0 : (std::uint64_t)(nbc * E));
+    nbk = (nv + E - 1) / E;
+    return b0;
+  };
+  uint4 r[MAXI];
+  std::int64_t be[kBwMaxBpt];
+  auto issue = [&](std::uint64_t ch) {
+    int nv, nbk;
+    const std::uint64_t b0 = blocks_of(ch, nv, nbk);
+#pragma unroll
+    for (int q = 0; q < kBwMaxBpt; ++q) {
+      const int b = tid + q * NT;
+      if (q < bpt && b < nbk) be[q] = load_exp(j.exps + (b0 + (std::uint64_t)b) * (std::uint64_t)(W / 8), W);
+    }
+    // whole blocks: the buffer holds every block in full
+    bw_issue<NT, MAXI>(j.words + b0 * (std::uint64_t)BB, (std::uint32_t)nbk * BB, r);
+  };
+  std::uint64_t ch = blockIdx.x;
+  if (bw_pipe<T>() && ch < nchunks) issue(ch);
+  for (; ch < nchunks; ch += gridDim.x) {
+    if (!bw_pipe<T>()) issue(ch);
+    int nv, nbk;
+    const std::uint64_t b0 = blocks_of(ch, nv, nbk);
     const std::uint8_t* gin = j.words + b0 * (std::uint64_t)BB;
-    std::uint8_t* gout = reinterpret_cast<std::uint8_t*>(y + v0);
+    std::uint8_t* gout = reinterpret_cast<std::uint8_t*>(y + b0 * (std::uint64_t)E);
     const std::uint32_t hw = (std::uint32_t)(reinterpret_cast<std::uintptr_t>(gin) & 15u);
     const std::uint32_t hv = (std::uint32_t)(reinterpret_cast<std::uintptr_t>(gout) & 15u);
-    // whole blocks: the buffer holds every block in full
-    chunk_copy<false>(const_cast<std::uint8_t*>(gin), s_img, (std::uint32_t)nbk * BB);
+    bw_commit<NT, MAXI>(gin, s_img, (std::uint32_t)nbk * BB, r);
+    std::int64_t ecur[kBwMaxBpt];
+#pragma unroll
+    for (int q = 0; q < kBwMaxBpt; ++q) ecur[q] = be[q];
     __syncthreads();
+    if (bw_pipe<T>() && ch + gridDim.x < nchunks) issue(ch + gridDim.x); // in flight while this chunk decodes
 
-    for (int b = tid; b < nbk; b += NT) {
-      const std::int64_t e = load_exp(j.exps + (b0 + (std::uint64_t)b) * (std::uint64_t)(W / 8), W);
+#pragma unroll
+    for (int q = 0; q < kBwMaxBpt; ++q) {
+      const int b = tid + q * NT;
+      if (q >= bpt || b >= nbk) break;
+      const std::int64_t e = ecur[q];
       const Word* src = reinterpret_cast<const Word*>(s_img + hw + (std::uint32_t)b * BB);
       Word wd[NWMAX];
 #pragma unroll
@@ -214,34 +359,57 @@ __global__ void __launch_bounds__(bw_threads<T>()) k_decompress_blockwise(Job j)
       }
       const int cnt = min(E, nv - b * E);
       T* sv = reinterpret_cast<T*>(s_val + hv) + b * E;
-      const bool plain = plain_exponent<T>(e);
-      const T inv = pow2<T>(plain ? (int)e - BITS + 2 : 0);
-      const U zero_bits = sizeof(T) == 4 ? (U)((std::uint32_t)(e + 96) << 23) : (U)((std::uint64_t)(e + 992) << 52);
+      // one loop per arithmetic, so only the block's own runs
+      auto unpack = [&](auto decode) {
 #pragma unroll
-      for (int k = 0; k < kBwMaxE; ++k) {
-        if (k >= cnt) break;
-        const int p = k * BITS, w = p / W, o = p % W; // compile-time after unrolling
-        C c = (C)((C)wd[w] >> o);
-        if (o + BITS > W) c |= (C)((C)wd[w + 1] << (W - o));
-        c &= CMASK;
-        const U r = plain ? decode_plain<T, BITS>(c, inv, zero_bits) : to_bits<T>(from_code<T>((U)c, e, BITS));
-        sv[k] = from_bits<T>(r);
+        for (int k = 0; k < kBwMaxE; ++k) {
+          if (k >= cnt) break;
+          const int p = k * BITS, w = p / W, o = p % W; // compile-time after unrolling
+          C c = (C)((C)wd[w] >> o);
+          if (o + BITS > W) c |= (C)((C)wd[w + 1] << (W - o));
+          sv[k] = from_bits<T>(decode((C)(c & CMASK)));
+        }
+      };
+      if (plain_exponent<T>(e)) {
+        const T inv = pow2<T>((int)e - BITS + 2);
+        const U zero_bits =
+          sizeof(T) == 4 ? (U)((std::uint32_t)(e + 96) << 23) : (U)((std::uint64_t)(e + 992) << 52);
+        unpack([&](C c) { return decode_plain<T, BITS>(c, inv, zero_bits); });
+      } else {
+        unpack([&](C c) { return to_bits<T>(from_code<T>((U)c, e, BITS)); });
       }
     }
     __syncthreads();
     chunk_copy<true>(gout, s_val, (std::uint32_t)nv * (std::uint32_t)sizeof(T));
-    __syncthreads(); // shared memory is reused by the next chunk
+    // no barrier here: the next chunk's commit writes the image region,
+    // which every thread finished reading before the barrier above
   }
 }
 
-// Launch of one width: one CTA per chunk (the loop covers any grid).
+// Launch of one width: a persistent grid of the resident CTAs (each CTA
+// overlaps the next chunk's loads with the current chunk's work), fewer when
+// there are fewer chunks.
 template<class T, int BITS>
 cudaError_t launch_blockwise_one(bool compress, const Job& j, cudaStream_t s)
 {
+  const std::size_t smem = bw_smem_bytes<T>(j.E);
+  // resident CTAs per SM by direction and block size (a benign race: every
+  // writer stores the same value)
+  static int resident[2][kBwMaxE + 1];
+  int& per_sm = resident[compress ? 0 : 1][j.E];
+  if (per_sm == 0) {
+    int n = 0;
+    const cudaError_t e =
+      compress ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_compress_blockwise<T, BITS>, bw_threads<T>(), smem)
+               : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_decompress_blockwise<T, BITS>, bw_threads<T>(),
+                                                               smem);
+    if (e != cudaSuccess) return e;
+    per_sm = n < 1 ? 1 : n;
+  }
   const std::uint64_t nb = (j.n + (std::uint64_t)j.E - 1) / (std::uint64_t)j.E;
   const std::uint64_t nbc = (std::uint64_t)bw_threads<T>() * (std::uint64_t)bw_bpt<T>(j.E);
-  const unsigned grid = (unsigned)std::max<std::uint64_t>(1, std::min<std::uint64_t>((nb + nbc - 1) / nbc, 1u << 30));
-  const std::size_t smem = bw_smem_bytes<T>(j.E);
+  const std::uint64_t ctas = (std::uint64_t)sm_count() * (std::uint64_t)per_sm;
+  const unsigned grid = (unsigned)std::max<std::uint64_t>(1, std::min<std::uint64_t>((nb + nbc - 1) / nbc, ctas));
   if (compress)
     k_compress_blockwise<T, BITS><<<grid, bw_threads<T>(), smem, s>>>(j);
   else
