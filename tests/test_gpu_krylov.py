@@ -66,3 +66,49 @@ def test_dot_with_w_not_32_byte_aligned(cuda):
     assert w.data_ptr() % 32 != 0
     h = basis.dot(w)
     assert torch.all((h - V @ w).abs() <= TOL * (V.abs() @ w.abs()) + 1e-300)
+
+
+def edge_vector(n, E, seed):
+    """Blocks whose exponents sit at the edges of the fused kernels' decode
+    ranges (1002 / 1003 / 1023 at the top, -959 / -960 / -1000 at the
+    bottom, 0), with zeros (zero codes), negative values and subnormals."""
+    rng = np.random.default_rng(seed)
+    x = np.empty(n, dtype=np.float64)
+    exps = (1002, 1003, 1023, -959, -960, -1000, 0, 5, -3)
+    for b in range(n // E):
+        be = exps[(b + seed) % len(exps)]
+        v = rng.uniform(-1.0, 1.0, E) * 2.0 ** be
+        v[rng.integers(E)] = (1.0 + rng.random()) * 2.0 ** be * (1 if rng.random() < 0.5 else -1)
+        v[rng.random(E) < 0.2] = 0.0
+        if be <= -959:
+            v[rng.random(E) < 0.1] = 5e-324 * rng.integers(1, 1000)
+        x[b * E:(b + 1) * E] = v
+    return x
+
+
+@pytest.mark.parametrize("bits", [16, 21, 24, 32, 48])
+def test_axpy_bit_exact_at_exponent_edges(cuda, bits):
+    """y[i] = fma(c[j], V[j][i], y[i]) for j = 0 .. m-1, each rounded once:
+    the fused axpy (which builds values of widths up to 32 bits without an
+    integer-to-double conversion in the blocks whose exponent lies in
+    [-959, 1002], and decodes the others as decompress does) equals that
+    sequence bit for bit, computed here exactly with rationals."""
+    from fractions import Fraction
+
+    n, m, E = 2048, 3, 32
+    basis = CompressedBasis(m, n, bits=bits, block_size=E)
+    for j in range(m):
+        basis.append(torch.from_numpy(edge_vector(n, E, 11 * j + bits)).cuda())
+    V = torch.stack([basis.get(j) for j in range(m)]).cpu().numpy()
+    rng = np.random.default_rng(bits)
+    c = rng.uniform(0.25, 0.5, m) * np.where(rng.random(m) < 0.5, -1.0, 1.0)
+    y0 = rng.standard_normal(n)
+    y = torch.from_numpy(y0).cuda()
+    basis.axpy(torch.from_numpy(c).cuda(), y)
+    want = y0.copy()
+    for j in range(m):
+        cj = Fraction(float(c[j]))
+        for i in range(n):
+            want[i] = float(cj * Fraction(float(V[j, i])) + Fraction(float(want[i])))
+    got = y.cpu().numpy()
+    assert np.array_equal(got.view(np.uint64), want.view(np.uint64))
