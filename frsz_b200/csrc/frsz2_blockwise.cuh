@@ -220,14 +220,17 @@ __global__ void __launch_bounds__(bw_threads<T>(), bw_min_ctas<T>()) k_compress_
       // Loops run to the block's count: fully unrolled (registers and bit
       // positions stay compile-time) with a branch out after value cnt - 1,
       // uniform across the warp except in the array's last block.
+      // raw keys doubled (the sign shifted out: a multiply, not a mask)
       U u[kBwMaxE];
-      std::uint32_t kr = 0;
+      std::uint32_t kr2 = 0;
 #pragma unroll
       for (int k = 0; k < kBwMaxE; ++k) {
         if (k >= cnt) break;
         u[k] = to_bits<T>(sv[k]);
-        kr = max(kr, K::raw(u[k]));
+        const std::uint32_t hi = sizeof(T) == 4 ? (std::uint32_t)u[k] : (std::uint32_t)((std::uint64_t)u[k] >> 32);
+        kr2 = max(kr2, hi * 2u);
       }
+      const std::uint32_t kr = kr2 >> 1;
       // block exponent: the largest non-NaN magnitude's (std::max semantics)
       std::uint32_t kc = kr;
       if (kr >= K::SPECIAL) {
@@ -242,7 +245,12 @@ __global__ void __launch_bounds__(bw_threads<T>(), bw_min_ctas<T>()) k_compress_
       const std::int64_t be = wrap_signed(ex, W);
       const bool plain = kr < K::SPECIAL && be == ex && plain_exponent<T>(be);
       const T scale = pow2<T>(plain ? BITS - 2 - (int)be : 0);
-      Word acc[NWMAX];
+      // Words of up to 32 bits are built in 32-bit registers (a narrower
+      // store keeps the low bits) and a code is added at its position,
+      // c * 2^o + acc, which equals the OR since the bits do not overlap and
+      // runs as one multiply-add instead of a shift and an OR.
+      using Acc = std::conditional_t<(W <= 32), std::uint32_t, std::uint64_t>;
+      Acc acc[NWMAX];
 #pragma unroll
       for (int w = 0; w < NWMAX; ++w) acc[w] = 0;
       // one loop per arithmetic, so only the block's own runs
@@ -252,8 +260,11 @@ __global__ void __launch_bounds__(bw_threads<T>(), bw_min_ctas<T>()) k_compress_
           if (k >= cnt) break;
           const C c = encode(u[k]);
           const int p = k * BITS, w = p / W, o = p % W; // compile-time after unrolling
-          acc[w] |= (Word)(c << o);
-          if (o + BITS > W) acc[w + 1] |= (Word)(c >> (W - o));
+          if constexpr (W <= 32)
+            acc[w] = (std::uint32_t)c * (1u << o) + acc[w];
+          else
+            acc[w] |= (Acc)c << o;
+          if (o + BITS > W) acc[w + 1] |= (Acc)(c >> (W - o));
         }
       };
       if (plain)
@@ -266,7 +277,7 @@ __global__ void __launch_bounds__(bw_threads<T>(), bw_min_ctas<T>()) k_compress_
 #pragma unroll
       for (int w = 0; w < NWMAX; ++w) {
         if (w >= nw) break;
-        dst[w] = acc[w];
+        dst[w] = (Word)acc[w];
       }
       store_word(j.exps + (b0 + (std::uint64_t)b) * (std::uint64_t)(W / 8), (std::uint64_t)be, W);
     }
