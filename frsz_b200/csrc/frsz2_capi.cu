@@ -163,11 +163,6 @@ static int launch_compress_t(const Job& j, int dtype, cudaStream_t s, bool* used
     return cuda_status(sizeof(T) == 8 ? launch_blockwise_f64(j.bits, true, j, s)
                                       : launch_blockwise_f32(j.bits, true, j, s),
                        "compress launch");
-  } else if (j.E <= kChunkMaxECompress) {
-    if (j.bits <= 32)
-      k_compress_chunked<T, std::uint32_t><<<chunk_grid(j), kNT, 0, s>>>(j);
-    else
-      k_compress_chunked<T, std::uint64_t><<<chunk_grid(j), kNT, 0, s>>>(j);
   } else {
     const std::uint64_t nb = (j.n + (std::uint64_t)j.E - 1) / (std::uint64_t)j.E;
     k_compress_generic<T><<<grid_for(nb, kNT / 32), kNT, 0, s>>>(j);
