@@ -169,7 +169,6 @@ __global__ void __launch_bounds__(bw_threads<T>(), bw_min_ctas<T>()) k_compress_
   using K = key_of<T>;
   constexpr int W = Cfg::W;
   using Word = bw_word_t<W>;
-  constexpr int NWMAX = (kBwMaxE * BITS + W - 1) / W;
   extern __shared__ __align__(16) std::uint8_t s_chunk[];
 
   const T* __restrict__ x = static_cast<const T*>(j.values_in);
@@ -215,19 +214,21 @@ __global__ void __launch_bounds__(bw_threads<T>(), bw_min_ctas<T>()) k_compress_
       bw_issue<NT, MAXI>(gn, (std::uint32_t)nvn * (std::uint32_t)sizeof(T), r);
     }
     for (int b = tid; b < nbk; b += NT) {
-      const T* sv = reinterpret_cast<const T*>(s_val + hv) + b * E;
+      const T* __restrict__ sv = reinterpret_cast<const T*>(s_val + hv) + b * E;
       const int cnt = min(E, nv - b * E);
-      // Loops run to the block's count: fully unrolled (registers and bit
-      // positions stay compile-time) with a branch out after value cnt - 1,
-      // uniform across the warp except in the array's last block.
-      // raw keys doubled (the sign shifted out: a multiply, not a mask)
-      U u[kBwMaxE];
+      // Loops run to the block's count: fully unrolled (bit positions stay
+      // compile-time) with a branch out after value cnt - 1, uniform across
+      // the warp except in the array's last block.  Values are read from
+      // shared memory in each pass instead of being held in registers.
+      //
+      // pass 1: the block maximum of the raw keys, doubled (the sign shifted
+      // out: a multiply, not a mask)
       std::uint32_t kr2 = 0;
 #pragma unroll
       for (int k = 0; k < kBwMaxE; ++k) {
         if (k >= cnt) break;
-        u[k] = to_bits<T>(sv[k]);
-        const std::uint32_t hi = sizeof(T) == 4 ? (std::uint32_t)u[k] : (std::uint32_t)((std::uint64_t)u[k] >> 32);
+        const U u = to_bits<T>(sv[k]);
+        const std::uint32_t hi = sizeof(T) == 4 ? (std::uint32_t)u : (std::uint32_t)((std::uint64_t)u >> 32);
         kr2 = max(kr2, hi * 2u);
       }
       const std::uint32_t kr = kr2 >> 1;
@@ -238,47 +239,46 @@ __global__ void __launch_bounds__(bw_threads<T>(), bw_min_ctas<T>()) k_compress_
 #pragma unroll
         for (int k = 0; k < kBwMaxE; ++k) {
           if (k >= cnt) break;
-          kc = max(kc, K::clean(u[k]));
+          kc = max(kc, K::clean(to_bits<T>(sv[k])));
         }
       }
       const std::int64_t ex = exponent_of_field<T>((int)(kc >> K::FSHIFT));
       const std::int64_t be = wrap_signed(ex, W);
       const bool plain = kr < K::SPECIAL && be == ex && plain_exponent<T>(be);
       const T scale = pow2<T>(plain ? BITS - 2 - (int)be : 0);
-      // Words of up to 32 bits are built in 32-bit registers (a narrower
-      // store keeps the low bits) and a code is added at its position,
-      // c * 2^o + acc, which equals the OR since the bits do not overlap and
-      // runs as one multiply-add instead of a shift and an OR.
+      Word* __restrict__ dst = reinterpret_cast<Word*>(s_img + hw + (std::uint32_t)b * BB);
+      // pass 2: codes into words, each word stored once it is complete, the
+      // last (partial) one after the block's last value -- so only the words
+      // the block's values reach are written.  Words of up to 32 bits are
+      // built in a 32-bit register (a narrower store keeps the low bits) and a
+      // code is added at its position, c * 2^o + word, which equals the OR
+      // since the bits do not overlap and runs as one multiply-add instead of
+      // a shift and an OR.
       using Acc = std::conditional_t<(W <= 32), std::uint32_t, std::uint64_t>;
-      Acc acc[NWMAX];
-#pragma unroll
-      for (int w = 0; w < NWMAX; ++w) acc[w] = 0;
-      // one loop per arithmetic, so only the block's own runs
       auto pack = [&](auto encode) {
+        Acc cur = 0;
 #pragma unroll
-        for (int k = 0; k < kBwMaxE; ++k) {
-          if (k >= cnt) break;
-          const C c = encode(u[k]);
+        for (int k = 0; k <= kBwMaxE; ++k) {
           const int p = k * BITS, w = p / W, o = p % W; // compile-time after unrolling
+          if (k == kBwMaxE || k >= cnt) {
+            if (o != 0) dst[w] = (Word)cur;
+            break;
+          }
+          const C c = encode(to_bits<T>(sv[k]));
           if constexpr (W <= 32)
-            acc[w] = (std::uint32_t)c * (1u << o) + acc[w];
+            cur = (std::uint32_t)c * (1u << o) + cur;
           else
-            acc[w] |= (Acc)c << o;
-          if (o + BITS > W) acc[w + 1] |= (Acc)(c >> (W - o));
+            cur |= (Acc)c << o;
+          if (o + BITS >= W) {
+            dst[w] = (Word)cur;
+            cur = o + BITS > W ? (Acc)(c >> (W - o)) : Acc(0);
+          }
         }
       };
       if (plain)
         pack([&](U v) { return encode_plain<T, BITS>(v, scale); });
       else
         pack([&](U v) { return (C)to_code<T>(v, (std::int16_t)be, BITS); });
-      // only the words the block's values reach (the array's last block)
-      const int nw = (int)(written_block_bytes(cnt, BITS, W) / (W / 8));
-      Word* dst = reinterpret_cast<Word*>(s_img + hw + (std::uint32_t)b * BB);
-#pragma unroll
-      for (int w = 0; w < NWMAX; ++w) {
-        if (w >= nw) break;
-        dst[w] = (Word)acc[w];
-      }
       store_word(j.exps + (b0 + (std::uint64_t)b) * (std::uint64_t)(W / 8), (std::uint64_t)be, W);
     }
     __syncthreads();
