@@ -130,6 +130,9 @@ static cudaError_t try_fast(bool compress, const Job& j, cudaStream_t s)
   if (small_block_eligible(j, sizeof(T) == 8, values, j.words))
     return sizeof(T) == 8 ? launch_fast_small_f64(j.bits, j.E, compress, j, s, grid)
                           : launch_fast_small_f32(j.bits, j.E, compress, j, s, grid);
+  if (fast_mis_eligible(j, sizeof(T) == 8, values, j.words))
+    return sizeof(T) == 8 ? launch_fast_mis_f64(j.bits, compress, j, s, grid)
+                          : launch_fast_mis_f32(j.bits, compress, j, s, grid);
   return cudaErrorNotSupported;
 }
 

@@ -144,6 +144,93 @@ __device__ __forceinline__ void store_word_bounded(std::uint8_t* base, std::uint
   }
 }
 
+// ---------------------------------------------------------------- values off the 32-byte layout
+
+// A lane's 32 bytes of values (8 words) when the values pointer sits kw
+// words (1..7) past a 32-byte boundary: the lane loads its aligned segment
+// a[0..8) (a = its values rounded down), takes the words after it from the
+// next lane's segment by shuffles (lane 31, whose neighbour is in another
+// row, loads them itself), and rotates by kw with one compile-time case per
+// kw (kw is the same for every lane of a launch, so the switch does not
+// diverge).  `first` marks the array's first lane, whose aligned segment
+// would start before the array: it reads its own words one by one.  Every
+// lane of the warp takes part.
+__device__ __forceinline__ void ld_lane_mis(const std::uint32_t* a, int kw, bool first, std::uint32_t (&v)[8])
+{
+  const int lane = threadIdx.x & 31;
+  std::uint32_t c0[8];
+  if (!first) {
+    ld256_stream(a, c0);
+  } else {
+#pragma unroll
+    for (int i = 0; i < 8; ++i) c0[i] = 0;
+  }
+  auto take = [&](auto kc) {
+    constexpr int K = decltype(kc)::value;
+    std::uint32_t c1[K];
+#pragma unroll
+    for (int i = 0; i < K; ++i) {
+      const std::uint32_t nb = __shfl_down_sync(0xFFFFFFFFu, c0[i], 1);
+      c1[i] = lane == 31 ? __ldg(a + 8 + i) : nb;
+    }
+    if (first) {
+#pragma unroll
+      for (int i = 0; i < 8; ++i) v[i] = __ldg(a + K + i);
+    } else {
+#pragma unroll
+      for (int i = 0; i < 8; ++i) v[i] = i + K < 8 ? c0[i + K] : c1[i + K - 8];
+    }
+  };
+  switch (kw) {
+    case 1: take(std::integral_constant<int, 1>{}); break;
+    case 2: take(std::integral_constant<int, 2>{}); break;
+    case 3: take(std::integral_constant<int, 3>{}); break;
+    case 4: take(std::integral_constant<int, 4>{}); break;
+    case 5: take(std::integral_constant<int, 5>{}); break;
+    case 6: take(std::integral_constant<int, 6>{}); break;
+    default: take(std::integral_constant<int, 7>{}); break;
+  }
+}
+
+// The store counterpart: lane L's 8 words go to a[kw .. kw + 8) with a the
+// lane's values rounded down to 32 bytes.  Lanes 1..31 store their aligned
+// segment a[0..8) whole -- the previous lane's last kw words (by shuffles)
+// and their own first 8 - kw; lane 0 stores its first 8 - kw words one by
+// one (its segment starts in the previous row), lane 31 its last kw (they
+// belong to the next row's first segment).  Every lane of the warp takes
+// part.
+__device__ __forceinline__ void st_lane_mis(std::uint32_t* a, int kw, const std::uint32_t (&v)[8])
+{
+  const int lane = threadIdx.x & 31;
+  auto put = [&](auto kc) {
+    constexpr int K = decltype(kc)::value;
+    std::uint32_t seg[8];
+#pragma unroll
+    for (int i = 0; i < K; ++i) seg[i] = __shfl_up_sync(0xFFFFFFFFu, v[8 - K + i], 1);
+#pragma unroll
+    for (int i = K; i < 8; ++i) seg[i] = v[i - K];
+    if (lane != 0) {
+      st256_stream(a, seg);
+    } else {
+#pragma unroll
+      for (int i = K; i < 8; ++i) a[i] = seg[i];
+    }
+    if (lane == 31) {
+#pragma unroll
+      for (int i = 0; i < K; ++i) a[8 + i] = v[8 - K + i];
+    }
+  };
+  switch (kw) {
+    case 1: put(std::integral_constant<int, 1>{}); break;
+    case 2: put(std::integral_constant<int, 2>{}); break;
+    case 3: put(std::integral_constant<int, 3>{}); break;
+    case 4: put(std::integral_constant<int, 4>{}); break;
+    case 5: put(std::integral_constant<int, 5>{}); break;
+    case 6: put(std::integral_constant<int, 6>{}); break;
+    default: put(std::integral_constant<int, 7>{}); break;
+  }
+}
+
 // ---------------------------------------------------------------- bit fields
 
 #ifndef FRSZ2_PUT_BITS_MAD
@@ -416,7 +503,7 @@ __device__ __forceinline__ void load_lane_exps(const std::uint8_t* p, std::int64
 // stage_words<>::value words, 16-byte aligned.
 // more_tiles: whether the CTA runs another tile after this one (the shared
 // block maxima are then reused, so their readers must be done first).
-template<class T, int BITS, int NT, int RPW_, bool PAD = false, int ESM = 0>
+template<class T, int BITS, int NT, int RPW_, bool PAD = false, int ESM = 0, bool MIS = false>
 __device__ __forceinline__ void fast_compress_tile(const Job& j, std::uint64_t tile, std::uint32_t* s_rmax,
                                                    std::uint32_t* s_stage, bool more_tiles = true)
 {
@@ -441,13 +528,18 @@ __device__ __forceinline__ void fast_compress_tile(const Job& j, std::uint64_t t
     const int nbt = full ? TB : ((rem + E - 1) >> log2E);
     const std::uint64_t b0 = tile * (std::uint64_t)TB;
 
+    // MIS: values off the 32-byte layout by kw words (whole tiles only)
+    const int kw = MIS ? (int)((reinterpret_cast<std::uintptr_t>(x) & 31u) >> 2) : 0;
     U u[RPW][P];
 #pragma unroll
     for (int rr = 0; rr < RPW; ++rr) {
       const int idx = (rr * Cfg::WARPS + warp) * ROW + lane * P;
-      if (full || idx + P <= rem) {
+      if (MIS ? full : (full || idx + P <= rem)) {
         std::uint32_t v[8];
-        ld256_stream(x + e0 + idx, v);
+        if constexpr (MIS)
+          ld_lane_mis(reinterpret_cast<const std::uint32_t*>(x + e0 + idx) - kw, kw, e0 + idx == 0, v);
+        else
+          ld256_stream(x + e0 + idx, v);
 #pragma unroll
         for (int i = 0; i < P; ++i) {
           if constexpr (sizeof(T) == 4)
@@ -685,19 +777,19 @@ __device__ __forceinline__ void fast_compress_tile(const Job& j, std::uint64_t t
   }
 }
 
-template<class T, int BITS, int NT = kNT, int RPW = 2, bool PAD = false, int ESM = 0>
+template<class T, int BITS, int NT = kNT, int RPW = 2, bool PAD = false, int ESM = 0, bool MIS = false>
 __global__ void __launch_bounds__(NT) k_compress_fast(Job j)
 {
   __shared__ std::uint32_t s_rmax[2 * fast_cfg<T, BITS, NT, RPW>::ROWS];
   __shared__ __align__(16) std::uint32_t s_stage[stage_words<T, BITS, NT, RPW, ESM>::value];
   for (std::uint64_t tile = blockIdx.x; tile < j.tiles; tile += gridDim.x)
-    fast_compress_tile<T, BITS, NT, RPW, PAD, ESM>(j, tile, s_rmax, s_stage, tile + gridDim.x < j.tiles);
+    fast_compress_tile<T, BITS, NT, RPW, PAD, ESM, MIS>(j, tile, s_rmax, s_stage, tile + gridDim.x < j.tiles);
 }
 
 // ---------------------------------------------------------------- decompress
 
 // One tile of decompress.
-template<class T, int BITS, int NT, int RPW_, bool PAD = false, int ESM = 0>
+template<class T, int BITS, int NT, int RPW_, bool PAD = false, int ESM = 0, bool MIS = false>
 __device__ __forceinline__ void fast_decompress_tile(const Job& j, std::uint64_t tile)
 {
   using Cfg = fast_cfg<T, BITS, NT, RPW_, ESM>;
@@ -794,7 +886,7 @@ __device__ __forceinline__ void fast_decompress_tile(const Job& j, std::uint64_t
         }
       }
 
-      if (full || idx + P <= rem) {
+      if (MIS ? full : (full || idx + P <= rem)) {
         std::uint32_t v[8];
 #pragma unroll
         for (int i = 0; i < P; ++i) {
@@ -805,7 +897,13 @@ __device__ __forceinline__ void fast_decompress_tile(const Job& j, std::uint64_t
             v[2 * i + 1] = (std::uint32_t)(outb[i] >> 32);
           }
         }
-        st256_stream(y + e0 + idx, v);
+        if constexpr (MIS) {
+          // values off the 32-byte layout by kw words (whole tiles only)
+          const int kw = (int)((reinterpret_cast<std::uintptr_t>(y) & 31u) >> 2);
+          st_lane_mis(reinterpret_cast<std::uint32_t*>(y + e0 + idx) - kw, kw, v);
+        } else {
+          st256_stream(y + e0 + idx, v);
+        }
       } else {
         for (int i = 0; i < P && idx + i < rem; ++i) y[e0 + idx + i] = from_bits<T>(outb[i]);
       }
@@ -813,11 +911,11 @@ __device__ __forceinline__ void fast_decompress_tile(const Job& j, std::uint64_t
   }
 }
 
-template<class T, int BITS, int NT = kNT, int RPW = 2, bool PAD = false, int ESM = 0>
+template<class T, int BITS, int NT = kNT, int RPW = 2, bool PAD = false, int ESM = 0, bool MIS = false>
 __global__ void __launch_bounds__(NT) k_decompress_fast(Job j)
 {
   for (std::uint64_t tile = blockIdx.x; tile < j.tiles; tile += gridDim.x)
-    fast_decompress_tile<T, BITS, NT, RPW, PAD, ESM>(j, tile);
+    fast_decompress_tile<T, BITS, NT, RPW, PAD, ESM, MIS>(j, tile);
 }
 
 // Whether a job's exponent blocks end in pad bits (E * bits not a multiple of
@@ -842,6 +940,17 @@ __host__ inline bool fast_eligible(const Job& j, int dtype_is_f64, const void* v
   if (reinterpret_cast<std::uintptr_t>(values) % 32 != 0) return false;
   if (reinterpret_cast<std::uintptr_t>(words) % 32 != 0) return false;
   return true;
+}
+
+// Requirements of the MIS instances: those of the fast kernels, with the
+// values pointer aligned to the element size but not to 32 bytes (the words
+// pointer still 32-byte aligned).
+__host__ inline bool fast_mis_eligible(const Job& j, int dtype_is_f64, const void* values, const void* words)
+{
+  const std::uintptr_t v = reinterpret_cast<std::uintptr_t>(values);
+  if (v % 32 == 0 || v % (dtype_is_f64 ? 8 : 4) != 0) return false;
+  const void* aligned = reinterpret_cast<const void*>(v - v % 32);
+  return fast_eligible(j, dtype_is_f64, aligned, words);
 }
 
 // Requirements of the small-block instances (ESM = E < P values per lane):

@@ -48,6 +48,43 @@ constexpr auto make_fast_table(std::integer_sequence<int, I...>)
 cudaError_t launch_fast_f32(int bits, bool compress, const Job& j, cudaStream_t s, unsigned grid);
 cudaError_t launch_fast_f64(int bits, bool compress, const Job& j, cudaStream_t s, unsigned grid);
 
+// The same kernels for a values pointer off the 32-byte layout (MIS).
+template<class T, int BITS>
+cudaError_t launch_fast_mis_one(bool compress, const Job& j, cudaStream_t s, unsigned grid)
+{
+  if constexpr (!fast_cfg<T, BITS>::ALIGNED) {
+    if (job_padded(j)) {
+      if (compress)
+        k_compress_fast<T, BITS, kNT, 2, true, 0, true><<<grid, kNT, 0, s>>>(j);
+      else
+        k_decompress_fast<T, BITS, kNT, 2, true, 0, true><<<grid, kNT, 0, s>>>(j);
+      return cudaGetLastError();
+    }
+  }
+  if (compress)
+    k_compress_fast<T, BITS, kNT, 2, false, 0, true><<<grid, kNT, 0, s>>>(j);
+  else
+    k_decompress_fast<T, BITS, kNT, 2, false, 0, true><<<grid, kNT, 0, s>>>(j);
+  return cudaGetLastError();
+}
+
+template<class T, int LO, int... I>
+constexpr auto make_fast_mis_table(std::integer_sequence<int, I...>)
+{
+  return std::array<fast_fn, sizeof...(I)>{ &launch_fast_mis_one<T, LO + I>... };
+}
+
+#define FRSZ2_FAST_MIS_TABLE(T, LO, HI, NAME)                                                                       \
+  cudaError_t NAME(int bits, bool compress, const Job& j, cudaStream_t s, unsigned grid)                          \
+  {                                                                                                                \
+    static constexpr auto table = make_fast_mis_table<T, LO>(std::make_integer_sequence<int, HI - LO + 1>{});      \
+    if (bits < LO || bits > HI) return cudaErrorNotSupported;                                                      \
+    return table[bits - LO](compress, j, s, grid);                                                                 \
+  }
+
+cudaError_t launch_fast_mis_f32(int bits, bool compress, const Job& j, cudaStream_t s, unsigned grid);
+cudaError_t launch_fast_mis_f64(int bits, bool compress, const Job& j, cudaStream_t s, unsigned grid);
+
 // Blocks of E < P values (E = 1, 2 or 4 for fp32; 1 or 2 for fp64): one
 // instance per (width, E).
 template<class T, int BITS, int ESM>

@@ -147,6 +147,35 @@ def test_small_blocks_every_width(cuda, dtype, bits):
         assert np.array_equal(out[1:].cpu().numpy().view(uint), oracle.decompress(ref, n, dtype, bits, E).view(uint))
 
 
+@pytest.mark.parametrize("dtype,bits", [(np.float32, b) for b in range(4, 33)] + [(np.float64, b) for b in range(4, 65)])
+def test_values_off_32_bytes_every_width(cuda, dtype, bits):
+    """Values pointer 1..7 (fp32) or 1..3 (fp64) elements past a 32-byte
+    boundary with a 32-byte aligned buffer (the fast kernels' MIS instances):
+    several whole tiles, a partial last tile, special values; bytes and values
+    equal the oracle's, and decompress writes nothing outside its output."""
+    es = np.dtype(dtype).itemsize
+    P = 32 // es
+    tdt = torch.float32 if es == 4 else torch.float64
+    uint = np.uint32 if es == 4 else np.uint64
+    for E in (P, 32, 256):
+        k = 1 + (bits + E) % (P - 1)
+        n = (3 * 4096 if es == 4 else 3 * 2048) + 3 * E + 5
+        x = special_values(dtype, n, bits * 7 + E)
+        base = torch.zeros(n + 2 * P, dtype=tdt, device="cuda")
+        base[k:k + n] = torch.from_numpy(x).cuda()
+        size = frsz_b200.compressed_size(dtype, bits, E, n)
+        buf = torch.full((size,), 0x21, dtype=torch.uint8, device="cuda")
+        frsz_b200.compress(base[k:k + n], bits, E, out=buf)
+        ref = oracle.compress(x, bits, E, canary=0x21)
+        assert np.array_equal(buf.cpu().numpy(), ref), (bits, E, k)
+        out = torch.full((n + 2 * P,), -7.0, dtype=tdt, device="cuda")
+        frsz_b200.decompress(torch.from_numpy(ref).cuda(), n, dtype, bits, E, out=out[k:k + n])
+        got = out.cpu().numpy()
+        want = oracle.decompress(ref, n, dtype, bits, E)
+        assert np.array_equal(got[k:k + n].view(uint), want.view(uint)), (bits, E, k)
+        assert np.all(got[:k] == -7.0) and np.all(got[k + n:] == -7.0), (bits, E, k)
+
+
 @pytest.mark.parametrize("dtype,bits,E", [(np.float32, 16, 32), (np.float32, 21, 8), (np.float64, 40, 4),
                                           (np.float64, 21, 64), (np.float32, 13, 1)])
 def test_pointers_off_alignment(cuda, dtype, bits, E):
