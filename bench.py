@@ -63,6 +63,10 @@ WORKLOADS = {
     "normal_f64_2p24_b33_e32": ("normal", "float64", 1 << 24, 33, 32),
     "normal_f64_2p24_b5_e32": ("normal", "float64", 1 << 24, 5, 32),
     "normal_f32_2p25_b16_e5": ("normal", "float32", 1 << 25, 16, 5),
+    # values (and outputs) starting 1 element past a 32-byte boundary, as a
+    # tensor view such as x[1:] does: (kind, dtype, n, bits, E, offset)
+    "normal_f32_2p28_b16_e32_off1": ("normal", "float32", 1 << 28, 16, 32, 1),
+    "normal_f64_2p27_b21_e32_off1": ("normal", "float64", 1 << 27, 21, 32, 1),
 }
 DEFAULT_WORKLOAD = "field512_f32_b16_e32"
 BATCH_WORKLOADS = ("batched4096", "krylov100", "serving", "legacy_f32_2p28", "legacy_f64_2p27", "legacy_f32_2p25")
@@ -252,7 +256,7 @@ def cpu_reference_codec(x: np.ndarray, bits: int, E: int, threads: int, min_seco
 def run_reference_arm(args, rank: int, world: int) -> None:
     if rank != 0:
         return
-    kind, dtype, n, bits, E = WORKLOADS[args.workload]
+    kind, dtype, n, bits, E = WORKLOADS[args.workload][:5]
     threads = os.cpu_count() or 1
     sample = min(n, 1 << 24)
     x = make_input_host_sample(kind, dtype, n, args.seed, sample)
@@ -321,13 +325,21 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=torch.device("cuda", local_rank))
 
-    kind, dtype, n, bits, E = WORKLOADS[args.workload]
+    kind, dtype, n, bits, E = WORKLOADS[args.workload][:5]
     frsz_b200.lib()  # fail loudly if the library is missing
     x = make_input_cuda(kind, dtype, n, args.seed + rank)
     tdt = x.dtype
     size = frsz_b200.compressed_size(dtype, bits, E, n)
     buf = torch.zeros(size, dtype=torch.uint8, device="cuda")
-    y = torch.empty_like(x)
+    offset = WORKLOADS[args.workload][5] if len(WORKLOADS[args.workload]) > 5 else 0
+    if offset:
+        xb = torch.empty(n + offset, dtype=tdt, device="cuda")
+        xb[offset:] = x
+        del x
+        x = xb[offset:]
+        y = torch.empty(n + offset, dtype=tdt, device="cuda")[offset:]
+    else:
+        y = torch.empty_like(x)
     stream = torch.cuda.current_stream()
     per_launch = algorithmic_bytes(dtype, n, bits, E)
     step_bytes = 2 * per_launch
@@ -444,7 +456,8 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
         "data": "synthetic",
         "config": {"workload": args.workload, "dtype": dtype, "n": n, "bits": bits, "block_size": E,
                    "bytes_per_step": step_bytes, "l2": "inputs larger than L2, no flush",
-                   "parallelism": f"replicas x{world}"},
+                   "parallelism": f"replicas x{world}",
+                   **({"values_offset_elems": offset} if offset else {})},
         "compress_gbs": round(per_launch / (comp_avg / 1e3) / 1e9, 2),
         "decompress_gbs": round(per_launch / (decomp_avg / 1e3) / 1e9, 2),
         "compress_ms": round(comp_avg, 5), "decompress_ms": round(decomp_avg, 5),
