@@ -149,14 +149,24 @@ __global__ void __launch_bounds__(kDecBlocks) k_frsz1_decompress(const std::int1
   const std::uint64_t g0 = v0 + (std::uint64_t)tid * kLegacyBlock; // this thread's block
   const int len = g0 < n ? (int)((n - g0) < (std::uint64_t)kLegacyBlock ? n - g0 : (std::uint64_t)kLegacyBlock) : 0;
   T acc = (T)0;
+  // own codes: two 16-byte loads per chunk, issued one chunk ahead so their
+  // latency overlaps the previous chunk's sums
+  uint4 pa = make_uint4(0, 0, 0, 0), pb = pa;
+  auto fetch = [&](int c) {
+    if (OWN && vec && c + kDecChunk <= len) {
+      const uint4* p = reinterpret_cast<const uint4*>(in + g0 + c);
+      pa = __ldg(p);
+      pb = __ldg(p + 1);
+    }
+  };
+  fetch(0);
   for (int c = 0; c < kLegacyBlock; c += kDecChunk) {
-    // this chunk's codes: the block's own (two 16-byte loads of the thread's
-    // contiguous codes) or block 0's
+    // this chunk's codes: the block's own or block 0's
     std::int16_t qc[kDecChunk];
     if constexpr (OWN) {
       if (vec && c + kDecChunk <= len) {
-        const uint4* p = reinterpret_cast<const uint4*>(in + g0 + c);
-        const uint4 a = __ldg(p), b = __ldg(p + 1);
+        const uint4 a = pa, b = pb;
+        if (c + kDecChunk < kLegacyBlock) fetch(c + kDecChunk);
         const std::uint32_t w[8] = { a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w };
 #pragma unroll
         for (int k = 0; k < kDecChunk; ++k) qc[k] = (std::int16_t)(w[k / 2] >> (16 * (k % 2)));
