@@ -161,3 +161,26 @@ def test_gpu_plugin_equals_oracle(cuda):
         assert np.array_equal(dev_out.cpu().numpy().reshape(-1).view(uint), host_out.reshape(-1).view(uint))
     p.set_options({"frsz:epsilon": 0.0})
     assert p.compress(f)[0] == 2 and p.error_code == 2
+
+
+@pytest.mark.gpu
+def test_gpu_rounding_ties_and_edges(cuda):
+    """Ties of the quantizer's round-half-away, magnitudes past 2^52 (already
+    integers), signed zeros, subnormals and differences at the int16 limits,
+    in both float types: bit for bit against the oracle (C round)."""
+    rng = np.random.default_rng(17)
+    for dtype in (np.float32, np.float64):
+        k = rng.integers(-40_000, 40_000, 3000).astype(np.float64)
+        parts = [k + 0.5, k - 0.5, -(k + 0.5), k,                  # ties at epsilon 0.5 (step 1)
+                 np.array([0.5, -0.5, 1.5, -1.5, 2.5, -2.5, 0.49999997, -0.49999997, 0.0, -0.0]),
+                 np.array([2.0 ** 52, -(2.0 ** 52) - 2, 2.0 ** 53 + 2, 1e20, -1e20, 3e38, -3e38]),
+                 np.array([1e-40, -1e-45, 5e-324 if dtype == np.float64 else 1e-45]),
+                 np.array([32767.5, -32768.5, 32766.5, -32767.5, 65535.0, -65536.0])]
+        x = np.concatenate(parts).astype(dtype)
+        x = np.concatenate([x, np.cumsum(rng.choice([-32768.0, 32767.0, 32767.5, -32768.5], 600)).astype(dtype)])
+        t = torch.from_numpy(x).cuda()
+        for eps in (0.5, 0.25, 1e-3):
+            with np.errstate(over="ignore", invalid="ignore"):
+                want = oracle.frsz1_compress(x, eps)
+            got = legacy.compress(t, eps).cpu().numpy()
+            assert np.array_equal(got, want), (dtype, eps, np.nonzero(got != want)[0][:5])
