@@ -67,6 +67,7 @@ WORKLOADS = {
     # tensor view such as x[1:] does: (kind, dtype, n, bits, E, offset)
     "normal_f32_2p28_b16_e32_off1": ("normal", "float32", 1 << 28, 16, 32, 1),
     "normal_f64_2p27_b21_e32_off1": ("normal", "float64", 1 << 27, 21, 32, 1),
+    "normal_f64_2p25_b21_e32_off1": ("normal", "float64", 1 << 25, 21, 32, 1),
 }
 DEFAULT_WORKLOAD = "field512_f32_b16_e32"
 BATCH_WORKLOADS = ("batched4096", "krylov100", "serving", "legacy_f32_2p28", "legacy_f64_2p27", "legacy_f32_2p25")

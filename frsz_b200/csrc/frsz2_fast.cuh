@@ -155,6 +155,7 @@ __device__ __forceinline__ void store_word_bounded(std::uint8_t* base, std::uint
 // diverge).  `first` marks the array's first lane, whose aligned segment
 // would start before the array: it reads its own words one by one.  Every
 // lane of the warp takes part.
+template<bool EARLY>
 __device__ __forceinline__ void ld_lane_mis(const std::uint32_t* a, int kw, bool first, std::uint32_t (&v)[8])
 {
   const int lane = threadIdx.x & 31;
@@ -165,13 +166,26 @@ __device__ __forceinline__ void ld_lane_mis(const std::uint32_t* a, int kw, bool
 #pragma unroll
     for (int i = 0; i < 8; ++i) c0[i] = 0;
   }
+  // EARLY: lane 31's words past its segment are loaded together with the
+  // segment rather than after the shuffles (which wait for the segment).
+  // Measured on B200 with fp64 values off by 1-3 elements: compress 0.81 ->
+  // 0.93 of HBM at 32 bits, 0.80 -> 0.84 at 16, but 0.73 -> 0.68 at 21, so
+  // the caller enables it for the widths whose lane segments are word-aligned.
+  std::uint32_t ext[7];
+  if constexpr (EARLY) {
+#pragma unroll
+    for (int i = 0; i < 7; ++i) ext[i] = lane == 31 && i < kw ? __ldg(a + 8 + i) : 0u;
+  }
   auto take = [&](auto kc) {
     constexpr int K = decltype(kc)::value;
     std::uint32_t c1[K];
 #pragma unroll
     for (int i = 0; i < K; ++i) {
       const std::uint32_t nb = __shfl_down_sync(0xFFFFFFFFu, c0[i], 1);
-      c1[i] = lane == 31 ? __ldg(a + 8 + i) : nb;
+      if constexpr (EARLY)
+        c1[i] = lane == 31 ? ext[i] : nb;
+      else
+        c1[i] = lane == 31 ? __ldg(a + 8 + i) : nb;
     }
     if (first) {
 #pragma unroll
@@ -537,7 +551,7 @@ __device__ __forceinline__ void fast_compress_tile(const Job& j, std::uint64_t t
       if (MIS ? full : (full || idx + P <= rem)) {
         std::uint32_t v[8];
         if constexpr (MIS)
-          ld_lane_mis(reinterpret_cast<const std::uint32_t*>(x + e0 + idx) - kw, kw, e0 + idx == 0, v);
+          ld_lane_mis<Cfg::ALIGNED>(reinterpret_cast<const std::uint32_t*>(x + e0 + idx) - kw, kw, e0 + idx == 0, v);
         else
           ld256_stream(x + e0 + idx, v);
 #pragma unroll
