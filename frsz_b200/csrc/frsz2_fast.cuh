@@ -337,57 +337,6 @@ __device__ __forceinline__ void unpack_lane(const std::uint32_t (&seg)[N], C (&c
   }
 }
 
-// ---------------------------------------------------------------- keys
-
-// Block-max key of a value: the magnitude bits that decide the exponent
-// field (all of |x| for fp32, the high word of |x| for fp64).  A key at or
-// above KEY_SPECIAL means the block holds +-Inf or NaN.
-template<class T>
-struct key_of;
-template<>
-struct key_of<float>
-{
-  static constexpr std::uint32_t SPECIAL = 0x7F800000u;
-  static constexpr int FSHIFT = 23;
-  __device__ static std::uint32_t raw(std::uint32_t u) { return u & 0x7FFFFFFFu; }
-  __device__ static std::uint32_t clean(std::uint32_t u)
-  {
-    const std::uint32_t a = u & 0x7FFFFFFFu;
-    return a > 0x7F800000u ? 0u : a;
-  }
-};
-template<>
-struct key_of<double>
-{
-  static constexpr std::uint32_t SPECIAL = 0x7FF00000u;
-  static constexpr int FSHIFT = 20;
-  __device__ static std::uint32_t raw(std::uint64_t u) { return (std::uint32_t)(u >> 32) & 0x7FFFFFFFu; }
-  __device__ static std::uint32_t clean(std::uint64_t u)
-  {
-    const std::uint64_t a = u & 0x7FFFFFFFFFFFFFFFull;
-    return a > 0x7FF0000000000000ull ? 0u : (std::uint32_t)(a >> 32);
-  }
-};
-
-// Exponent range in which the float-arithmetic formulas are exact.
-template<class T>
-__device__ __forceinline__ bool plain_exponent(std::int64_t be)
-{
-  if constexpr (sizeof(T) == 4)
-    return be >= -95 && be <= 127;
-  else
-    return be >= -959 && be <= 1023;
-}
-
-template<class T>
-__device__ __forceinline__ T pow2(int e) // 2^e, e within the normal range
-{
-  if constexpr (sizeof(T) == 4)
-    return __uint_as_float((std::uint32_t)(e + 127) << 23);
-  else
-    return __longlong_as_double((long long)(e + 1023) << 52);
-}
-
 // ---------------------------------------------------------------- encode / decode
 
 template<class T, int BITS>

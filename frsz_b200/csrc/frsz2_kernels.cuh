@@ -109,6 +109,70 @@ __device__ __forceinline__ std::int64_t block_exponent(std::uint32_t field_max, 
   return wrap_signed(exponent_of_field<T>((int)field_max), W);
 }
 
+// ---------------------------------------------------------------- keys
+
+// Block-max key of a value: the magnitude bits that decide the exponent
+// field (all of |x| for fp32, the high word of |x| for fp64).  A key at or
+// above KEY_SPECIAL means the block holds +-Inf or NaN.
+template<class T>
+struct key_of;
+template<>
+struct key_of<float>
+{
+  static constexpr std::uint32_t SPECIAL = 0x7F800000u;
+  static constexpr int FSHIFT = 23;
+  __device__ static std::uint32_t raw(std::uint32_t u) { return u & 0x7FFFFFFFu; }
+  __device__ static std::uint32_t clean(std::uint32_t u)
+  {
+    const std::uint32_t a = u & 0x7FFFFFFFu;
+    return a > 0x7F800000u ? 0u : a;
+  }
+};
+template<>
+struct key_of<double>
+{
+  static constexpr std::uint32_t SPECIAL = 0x7FF00000u;
+  static constexpr int FSHIFT = 20;
+  __device__ static std::uint32_t raw(std::uint64_t u) { return (std::uint32_t)(u >> 32) & 0x7FFFFFFFu; }
+  __device__ static std::uint32_t clean(std::uint64_t u)
+  {
+    const std::uint64_t a = u & 0x7FFFFFFFFFFFFFFFull;
+    return a > 0x7FF0000000000000ull ? 0u : (std::uint32_t)(a >> 32);
+  }
+};
+
+// Exponent range in which the float-arithmetic formulas are exact.
+template<class T>
+__device__ __forceinline__ bool plain_exponent(std::int64_t be)
+{
+  if constexpr (sizeof(T) == 4)
+    return be >= -95 && be <= 127;
+  else
+    return be >= -959 && be <= 1023;
+}
+
+template<class T>
+__device__ __forceinline__ T pow2(int e) // 2^e, e within the normal range
+{
+  if constexpr (sizeof(T) == 4)
+    return __uint_as_float((std::uint32_t)(e + 127) << 23);
+  else
+    return __longlong_as_double((long long)(e + 1023) << 52);
+}
+
+// trunc(|x| * scale) with the sign at bit `bits` - 1, for a runtime width
+// (the plain-range arithmetic of encode_plain in frsz2_fast.cuh).
+template<class T>
+__device__ __forceinline__ std::uint64_t encode_plain_rt(typename fp<T>::U u, T scale, int bits)
+{
+  const T x = from_bits<T>(u);
+  const std::uint64_t s = (std::uint64_t)(u >> (fp<T>::UBITS - 1)) << (bits - 1);
+  if constexpr (sizeof(T) == 4)
+    return (std::uint64_t)__float2uint_rz(fabsf(x) * scale) | s;
+  else
+    return (std::uint64_t)__double2ull_rz(fabs(x) * scale) | s;
+}
+
 // ======================================================================
 // generic kernels: one warp per exponent block
 // ======================================================================
@@ -127,15 +191,27 @@ __global__ void __launch_bounds__(kNT) k_compress_generic(Job j)
   for (std::uint64_t b = warp; b < nb; b += nwarps) {
     const std::uint64_t base = b * (std::uint64_t)E;
     const int cnt = (int)((j.n - base) < (std::uint64_t)E ? (j.n - base) : (std::uint64_t)E);
-    std::uint32_t fmax = 0;
+    std::uint32_t fmax = 0, kraw = 0;
     for (int k = lane; k < cnt; k += 32) {
-      const std::uint32_t f = max_field<T>(load_bits(x + base + k));
+      const U u = load_bits(x + base + k);
+      const std::uint32_t f = max_field<T>(u);
       fmax = f > fmax ? f : fmax;
+      kraw = max(kraw, key_of<T>::raw(u));
     }
     fmax = __reduce_max_sync(0xFFFFFFFFu, fmax);
+    kraw = __reduce_max_sync(0xFFFFFFFFu, kraw);
+    const std::int64_t ex = exponent_of_field<T>((int)fmax);
     const std::int64_t be = block_exponent<T>(fmax, W);
     const int be16 = (std::int16_t)be;
     if (lane == 0) store_word(j.exps + b * (std::uint64_t)(W / 8), (std::uint64_t)be, W);
+    // the float arithmetic where it is exact (no Inf / NaN, no exponent wrap,
+    // plain range), else the integer restatement
+    const bool plain = kraw < key_of<T>::SPECIAL && be == ex && plain_exponent<T>(be);
+    const T scale = pow2<T>(plain ? bits - 2 - (int)be : 0);
+    auto code = [&](int k) -> std::uint64_t {
+      const U u = load_bits(x + base + k);
+      return plain ? encode_plain_rt<T>(u, scale, bits) : (std::uint64_t)to_code<T>(u, be16, bits);
+    };
 
     // word w holds stream bits [w*W, w*W + W); only the words the reference
     // writes for `cnt` values are stored
@@ -145,10 +221,10 @@ __global__ void __launch_bounds__(kNT) k_compress_generic(Job j)
       const std::int64_t pos = (std::int64_t)w * W;
       int k = (int)(pos / bits);
       const int off = (int)(pos - (std::int64_t)k * bits);
-      std::uint64_t acc = (std::uint64_t)to_code<T>(load_bits(x + base + k), be16, bits) >> off;
+      std::uint64_t acc = code(k) >> off;
       int have = bits - off;
       for (++k; have < W && k < cnt; ++k) {
-        acc |= (std::uint64_t)to_code<T>(load_bits(x + base + k), be16, bits) << have;
+        acc |= code(k) << have;
         have += bits;
       }
       store_word(wbase + (std::uint64_t)w * (W / 8), acc, W);
