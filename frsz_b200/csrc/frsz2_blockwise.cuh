@@ -22,6 +22,7 @@
 
 #include <algorithm>
 #include <array>
+#include <atomic>
 #include <utility>
 
 namespace frsz2b {
@@ -404,10 +405,11 @@ template<class T, int BITS>
 cudaError_t launch_blockwise_one(bool compress, const Job& j, cudaStream_t s)
 {
   const std::size_t smem = bw_smem_bytes<T>(j.E);
-  // resident CTAs per SM by direction and block size (a benign race: every
-  // writer stores the same value)
-  static int resident[2][kBwMaxE + 1];
-  int& per_sm = resident[compress ? 0 : 1][j.E];
+  // resident CTAs per SM by direction and block size, queried once (threads
+  // racing on the first call all store the same value)
+  static std::atomic<int> resident[2][kBwMaxE + 1];
+  std::atomic<int>& slot = resident[compress ? 0 : 1][j.E];
+  int per_sm = slot.load(std::memory_order_relaxed);
   if (per_sm == 0) {
     int n = 0;
     const cudaError_t e =
@@ -416,6 +418,7 @@ cudaError_t launch_blockwise_one(bool compress, const Job& j, cudaStream_t s)
                                                                smem);
     if (e != cudaSuccess) return e;
     per_sm = n < 1 ? 1 : n;
+    slot.store(per_sm, std::memory_order_relaxed);
   }
   const std::uint64_t nb = (j.n + (std::uint64_t)j.E - 1) / (std::uint64_t)j.E;
   const std::uint64_t nbc = (std::uint64_t)bw_threads<T>() * (std::uint64_t)bw_bpt<T>(j.E);

@@ -9,6 +9,7 @@
 #include "../../include/frsz2_b200.h"
 
 #include <algorithm>
+#include <atomic>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -47,15 +48,17 @@ int check_args(int dtype, int bits, int E)
 
 int sm_count()
 {
-  static int cached[64] = { 0 };
+  // per device, queried once (threads racing on the first call store the
+  // same value)
+  static std::atomic<int> cached[64];
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148;
-  if (cached[dev] == 0) {
-    int c = 0;
+  int c = cached[dev].load(std::memory_order_relaxed);
+  if (c == 0) {
     if (cudaDeviceGetAttribute(&c, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || c <= 0) c = 148;
-    cached[dev] = c;
+    cached[dev].store(c, std::memory_order_relaxed);
   }
-  return cached[dev];
+  return c;
 }
 
 static bool is_pow2(int x) { return x > 0 && (x & (x - 1)) == 0; }
