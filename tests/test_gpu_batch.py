@@ -131,3 +131,30 @@ def test_batch_padded_and_unpadded_blocks_in_one_class(cuda):
     torch.cuda.synchronize()
     check_batch(arrays, host)
     plan.close()
+
+
+def test_batch_views_off_32_bytes(cuda):
+    """Arrays whose values and outputs are views 1-3 elements past a 32-byte
+    boundary (element-aligned) run as separate launches inside the plan's
+    graph, on the fast kernels' instances for such views; the results equal
+    the oracle's."""
+    specs = [(np.float32, 3 * 4096 + 17, 16, 32, 1), (np.float64, 2 * 2048 + 5, 21, 64, 3),
+             (np.float32, 9_000, 12, 8, 2), (np.float64, 5_000, 40, 16, 1), (np.float32, 4096, 16, 32, 0)]
+    arrays, host = [], []
+    for k, (dtype, n, bits, E, off) in enumerate(specs):
+        x = workloads.loguniform_np(n, dtype, seed=70 + k, lo=-12, hi=12)
+        tdt = torch.float32 if dtype == np.float32 else torch.float64
+        base = torch.zeros(n + 8, dtype=tdt, device="cuda")
+        base[off:off + n] = torch.from_numpy(x).cuda()
+        out = torch.full((n + 8,), float("nan"), dtype=tdt, device="cuda")
+        buf = torch.full((frsz_b200.compressed_size(dtype, bits, E, n),), 0x3D, dtype=torch.uint8, device="cuda")
+        arrays.append(BatchArray(values=base[off:off + n], compressed=buf, bits=bits, block_size=E,
+                                 decompressed=out[off:off + n]))
+        host.append(x)
+    plan = BatchPlan(arrays)
+    assert plan.info()["separate_launches"] == 4
+    plan.compress()
+    plan.decompress()
+    torch.cuda.synchronize()
+    check_batch(arrays, host)
+    plan.close()
