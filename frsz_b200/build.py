@@ -23,7 +23,8 @@ SOURCES = ["frsz2_capi.cu", "frsz2_fast_f32.cu", "frsz2_fast_f64.cu", "frsz2_fas
            "frsz2_fast_small_f64.cu", "frsz2_batch.cu", "frsz2_batch_f32.cu",
            "frsz2_batch_f64.cu", "frsz2_batch_static.cu", "frsz2_krylov.cu",
            "frsz2_serve.cu", "frsz1_legacy.cu", "frsz2_blockwise_f32.cu", "frsz2_blockwise_f64.cu",
-           "frsz2_fast_mis_f32.cu", "frsz2_fast_mis_f64.cu"]
+           "frsz2_fast_mis_f32.cu", "frsz2_fast_mis_f64.cu",
+           "frsz2_blockvec_f32.cu", "frsz2_blockvec_f64.cu"]
 OBJDIR = os.path.join(HERE, "_build")
 
 

@@ -1,5 +1,6 @@
 // frsz2_capi.cu -- C ABI of libfrsz2_b200.so: argument checks, kernel choice,
 // launch geometry, and the host-buffer path with pipelined copies.
+#include "frsz2_blockvec.cuh"
 #include "frsz2_blockwise.cuh"
 #include "frsz2_chunked.cuh"
 #include "frsz2_fast_dispatch.hpp"
@@ -140,6 +141,20 @@ static cudaError_t try_fast(bool compress, const Job& j, cudaStream_t s)
 }
 
 
+// The blocks of a job from block b0 on (the generic kernel's share when the
+// blockvec kernel takes the whole blocks).
+static Job job_from_block(const Job& j, std::uint64_t b0, std::size_t es)
+{
+  Job t = j;
+  const std::uint64_t e0 = b0 * (std::uint64_t)j.E;
+  t.n = j.n - e0;
+  if (j.values_in) t.values_in = static_cast<const std::uint8_t*>(j.values_in) + e0 * es;
+  if (j.values_out) t.values_out = static_cast<std::uint8_t*>(j.values_out) + e0 * es;
+  t.exps = j.exps + b0 * (std::uint64_t)(j.W / 8);
+  t.words = j.words + b0 * (std::uint64_t)j.block_bytes;
+  return t;
+}
+
 // One CTA per chunk of whole blocks (frsz2_chunked.cuh).
 static unsigned chunk_grid(const Job& j)
 {
@@ -169,6 +184,12 @@ static int launch_compress_t(const Job& j, int dtype, cudaStream_t s, bool* used
     return cuda_status(sizeof(T) == 8 ? launch_blockwise_f64(j.bits, true, j, s)
                                       : launch_blockwise_f32(j.bits, true, j, s),
                        "compress launch");
+  } else if (blockvec_eligible(j, sizeof(T), j.values_in, j.words)) {
+    const std::uint64_t full = j.n / (std::uint64_t)j.E;
+    const cudaError_t e = sizeof(T) == 8 ? launch_blockvec_f64(j.bits, j, full, s)
+                                         : launch_blockvec_f32(j.bits, j, full, s);
+    if (e != cudaSuccess) return cuda_status(e, "compress launch");
+    if (full * (std::uint64_t)j.E < j.n) k_compress_generic<T><<<1, kNT, 0, s>>>(job_from_block(j, full, sizeof(T)));
   } else {
     const std::uint64_t nb = (j.n + (std::uint64_t)j.E - 1) / (std::uint64_t)j.E;
     k_compress_generic<T><<<grid_for(nb, kNT / 32), kNT, 0, s>>>(j);

@@ -27,8 +27,10 @@
  * Speed: power-of-two block sizes from 8 (fp32) / 4 (fp64) values up with a
  * 32-byte aligned buffer run at about the HBM bandwidth; values off the
  * 32-byte layout (a view such as x + 1) at 0.7-0.9 of it; other block sizes
- * up to 16 values at 0.4-0.8; larger block sizes that are not powers of two,
- * or a buffer off the 32-byte layout, on slower general kernels.
+ * up to 16 values at 0.4-0.8; compress of block sizes 17-64 whose blocks
+ * start on 16-byte boundaries at 0.2-0.7; other block sizes that are not
+ * powers of two, or a buffer off the 32-byte layout, on slower general
+ * kernels.
  */
 #ifndef FRSZ2_B200_H
 #define FRSZ2_B200_H

@@ -147,6 +147,19 @@ def test_small_blocks_every_width(cuda, dtype, bits):
         assert np.array_equal(out[1:].cpu().numpy().view(uint), oracle.decompress(ref, n, dtype, bits, E).view(uint))
 
 
+@pytest.mark.parametrize("dtype,bits", [(np.float32, b) for b in range(4, 33)] + [(np.float64, b) for b in range(4, 33)])
+def test_blocks_17_to_64_every_width(cuda, dtype, bits):
+    """Block sizes 17..64 that are not powers of two with 16-byte block
+    starts (compress on the blockvec kernel: block bytes a multiple of 16 or
+    only of 4, the partial last block on the generic kernel; decompress on
+    the chunked kernel), special values."""
+    Es = (20, 24, 36, 44, 48, 60) if dtype == np.float32 else (18, 22, 24, 34, 48, 62)
+    for E in Es:
+        n = 700 * E + E // 3 + 1
+        x = special_values(dtype, n, bits * 13 + E)
+        check(x, bits, E)
+
+
 @pytest.mark.parametrize("dtype,bits", [(np.float32, b) for b in range(4, 33)] + [(np.float64, b) for b in range(4, 65)])
 def test_values_off_32_bytes_every_width(cuda, dtype, bits):
     """Values pointer 1..7 (fp32) or 1..3 (fp64) elements past a 32-byte
