@@ -63,6 +63,7 @@ WORKLOADS = {
     "normal_f64_2p24_b33_e32": ("normal", "float64", 1 << 24, 33, 32),
     "normal_f64_2p24_b5_e32": ("normal", "float64", 1 << 24, 5, 32),
     "normal_f32_2p25_b16_e5": ("normal", "float32", 1 << 25, 16, 5),
+    "normal_f32_2p28_b16_e24": ("normal", "float32", 1 << 28, 16, 24),
     # values (and outputs) starting 1 element past a 32-byte boundary, as a
     # tensor view such as x[1:] does: (kind, dtype, n, bits, E, offset)
     "normal_f32_2p28_b16_e32_off1": ("normal", "float32", 1 << 28, 16, 32, 1),
