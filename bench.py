@@ -1,10 +1,13 @@
 #!/usr/bin/env python
 """FRSZ2 compress/decompress throughput on B200.
 
-Default workload (the configuration the headline metric is quoted on): an fp32
-512^3 field (sum of 8 random-phase plane sinusoids, wavelengths 8-256 cells,
-plus N(0, 1e-3) noise), exponent block 32, 16 bits per value.  One step =
-compress the whole field into its FRSZ2 buffer, then decompress it back.
+Default workload: the 2 GiB fp64 array (2^28 values, random sign, magnitude
+10^U(-30, 30), 1 % exact zeros, 0.1 % subnormals), exponent block 32, 21 bits
+per value -- the single-array configuration with the 70 %-of-HBM target, at
+its unaligned width.  One step = compress the whole array into its FRSZ2
+buffer, then decompress it back.  The same line carries the other five cases
+of that configuration (blocks of 32 and 64 at 16 / 21 / 32 bits), each timed
+the same way on the same array, under "cases".
 
   value     whole-job GB/s of algorithmic bytes (compress: values read + exps
             and words written; decompress: the reverse; the 256 B pad is not
@@ -15,10 +18,11 @@ compress the whole field into its FRSZ2 buffer, then decompress it back.
   roofline  the dominant kernel's algorithmic GB/s over the measured HBM copy
             bandwidth
   cpu_baseline  the reference's own CPU codec (oracle/_ref, all host threads)
-            on a bounded sample of the same workload
+            on the same whole array
 
 ``--impl reference`` times that reference CPU codec alone on the same
-workload and prints the reference-arm line.  Under torchrun every rank
+workload (the whole array, the same values) and prints the reference-arm
+line.  Under torchrun every rank
 compresses its own field (weak scaling, no data-path collective); the timing
 is the max over ranks.
 """
@@ -70,7 +74,9 @@ WORKLOADS = {
     "normal_f64_2p27_b21_e32_off1": ("normal", "float64", 1 << 27, 21, 32, 1),
     "normal_f64_2p25_b21_e32_off1": ("normal", "float64", 1 << 25, 21, 32, 1),
 }
-DEFAULT_WORKLOAD = "field512_f32_b16_e32"
+DEFAULT_WORKLOAD = "loguniform_f64_2p28_b21_e32"
+# the six cases of the 2 GiB fp64 configuration: (bits, block size)
+F64_2P28_CASES = ((16, 32), (21, 32), (32, 32), (16, 64), (21, 64), (32, 64))
 BATCH_WORKLOADS = ("batched4096", "krylov100", "serving", "legacy_f32_2p28", "legacy_f64_2p27", "legacy_f32_2p25")
 
 # DRAM bytes (read + write) per launch from ncu captures, by (workload, kernel);
@@ -197,12 +203,16 @@ def make_input_cuda(kind: str, dtype: str, n: int, seed: int):
         side = round(n ** (1 / 3))
         return workloads.sinusoid_field_cuda(side, side, side, seed=seed, dtype=tdt)
     if kind == "loguniform":
-        return workloads.loguniform_cuda(n, tdt, seed=seed)
+        # generated on the host, as the reference arm does: both arms code the same values
+        npdt = np.float32 if dtype == "float32" else np.float64
+        return torch.from_numpy(workloads.loguniform_host(n, npdt, seed=seed)).to("cuda")
     return workloads.normal_cuda(n, tdt, seed=seed)
 
 
-def make_input_host_sample(kind: str, dtype: str, n: int, seed: int, sample: int) -> np.ndarray:
-    """The first `sample` values of the workload, generated on the host."""
+def make_input_host(kind: str, dtype: str, n: int, seed: int) -> np.ndarray:
+    """The workload's values generated on the host (the same values as
+    make_input_cuda for the log-uniform arrays; the field and the normal
+    arrays come from the host generators of the same distributions)."""
     import torch
 
     from frsz_b200 import workloads
@@ -210,12 +220,11 @@ def make_input_host_sample(kind: str, dtype: str, n: int, seed: int, sample: int
     npdt = np.float32 if dtype == "float32" else np.float64
     if kind == "field":
         side = round(n ** (1 / 3))
-        nz = max(1, -(-sample // (side * side)))
-        f = workloads.sinusoid_field_cuda(side, side, nz, seed=seed, dtype=torch.float32, device="cpu")
-        return f.numpy().astype(npdt)[:sample]
+        f = workloads.sinusoid_field_cuda(side, side, side, seed=seed, dtype=torch.float32, device="cpu")
+        return f.numpy().astype(npdt)
     if kind == "loguniform":
-        return workloads.loguniform_np(sample, npdt, seed=seed)
-    return workloads.normal_np(sample, npdt, seed=seed)
+        return workloads.loguniform_host(n, npdt, seed=seed)
+    return workloads.normal_np(n, npdt, seed=seed)
 
 
 # ---------------------------------------------------------------- CPU reference codec
@@ -256,61 +265,83 @@ def cpu_reference_codec(x: np.ndarray, bits: int, E: int, threads: int, min_seco
 # ---------------------------------------------------------------- reference arm
 
 def run_reference_arm(args, rank: int, world: int) -> None:
+    """The reference's own CPU codec (frsz2.hpp's compress_cpu_block /
+    decompress_cpu_block over block ranges split across all host threads,
+    built from the reference sources into oracle/_ref) on the whole workload:
+    one step = compress + decompress of every value, as in our arm."""
     if rank != 0:
         return
     kind, dtype, n, bits, E = WORKLOADS[args.workload][:5]
     threads = os.cpu_count() or 1
-    sample = min(n, 1 << 24)
-    x = make_input_host_sample(kind, dtype, n, args.seed, sample)
+    x = make_input_host(kind, dtype, n, args.seed)
     import oracle
 
     impl_kind = "reference" if oracle.ref_available() else "port"
     buf = np.zeros(oracle.compressed_bytes(bits, E, x.size), dtype=np.uint8)
     y = np.empty_like(x)
 
-    def step(xs, b, ys):
+    def step():
         if impl_kind == "reference":
-            oracle.ref_compress_into(xs, b, bits, E, threads)
-            oracle.ref_decompress_into(b, ys, bits, E, threads)
+            oracle.ref_compress_into(x, buf, bits, E, threads)
+            oracle.ref_decompress_into(buf, y, bits, E, threads)
         else:
             lib = oracle.oracle_lib()
-            lib.frsz2o_compress_mt(int(xs.dtype == np.float64), xs.ctypes.data, xs.size, bits, E, b.ctypes.data,
+            lib.frsz2o_compress_mt(int(x.dtype == np.float64), x.ctypes.data, x.size, bits, E, buf.ctypes.data,
                                    threads)
-            lib.frsz2o_decompress_mt(int(xs.dtype == np.float64), b.ctypes.data, xs.size, bits, E, ys.ctypes.data,
+            lib.frsz2o_decompress_mt(int(x.dtype == np.float64), buf.ctypes.data, x.size, bits, E, y.ctypes.data,
                                      threads)
 
-    t0 = time.perf_counter()
     for _ in range(max(1, args.warmup)):
-        step(x, buf, y)
-    per = (time.perf_counter() - t0) / max(1, args.warmup)
-    # keep the whole timed run within about a minute
-    if per * args.steps > 60.0:
-        sample = max(1 << 18, int(sample * 60.0 / (per * args.steps)) // E * E)
-        x = x[:sample].copy()
-        buf = np.zeros(oracle.compressed_bytes(bits, E, x.size), dtype=np.uint8)
-        y = np.empty_like(x)
-        step(x, buf, y)
+        step()
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        step(x, buf, y)
+        step()
     dt = time.perf_counter() - t0
-    nbytes = 2 * algorithmic_bytes(dtype, x.size, bits, E)
+    nbytes = 2 * algorithmic_bytes(dtype, n, bits, E)
     value = nbytes * args.steps / dt / 1e9
     line = {
         "impl": "reference", "metric": METRIC, "value": round(value, 3), "unit": "GB/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(dt / args.steps * 1e3, 4),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "u32" if dtype == "float32" else "u64", "data": "synthetic",
-        "config": {"workload": args.workload, "dtype": dtype, "n": n, "bits": bits, "block_size": E,
-                   "sample_values": int(x.size)},
+        "config": {"workload": args.workload, "dtype": dtype, "n": n, "bits": bits, "block_size": E},
         "cpu_baseline": {"value": round(value, 3), "unit": "GB/s", "cores": threads, "kind": impl_kind,
-                         "sample": f"first {x.size} values of the workload, compress+decompress per step"},
+                         "sample": f"all {n} values of the workload, compress+decompress per step"},
         "e2e": {"value": round(value, 3), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
 
 
 # ---------------------------------------------------------------- our arm
+
+def time_case(x, y, bits: int, E: int, warmup: int, K: int, stream):
+    """Mean compress and decompress launch times (ms, CUDA events on the
+    launching stream) of one (bits, E) case on the resident array x, and the
+    number of values outside the per-block error bound."""
+    import torch
+
+    import frsz_b200
+
+    n = x.numel()
+    buf = torch.zeros(frsz_b200.compressed_size(x.dtype, bits, E, n), dtype=torch.uint8, device=x.device)
+    for _ in range(warmup):
+        frsz_b200.compress(x, bits, E, out=buf, stream=stream)
+        frsz_b200.decompress(buf, n, x.dtype, bits, E, out=y, stream=stream)
+    torch.cuda.synchronize()
+    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(K)]
+    for ev in evs:
+        ev[0].record(stream)
+        frsz_b200.compress(x, bits, E, out=buf, stream=stream)
+        ev[1].record(stream)
+        frsz_b200.decompress(buf, n, x.dtype, bits, E, out=y, stream=stream)
+        ev[2].record(stream)
+    torch.cuda.synchronize()
+    c_ms = statistics.mean(e[0].elapsed_time(e[1]) for e in evs)
+    d_ms = statistics.mean(e[1].elapsed_time(e[2]) for e in evs)
+    viol = error_report(x, y, buf, bits, E)["bound_violations"]
+    del buf
+    return c_ms, d_ms, viol
+
 
 def run_ours(args, rank: int, world: int, local_rank: int) -> None:
     import torch
@@ -393,6 +424,23 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
 
     value = world * step_bytes * K / (elapsed_ms / 1e3) / 1e9
     errors = error_report(x, y, buf, bits, E)
+    peaks = load_peaks()
+
+    # ---- the other cases of the 2 GiB fp64 configuration, same array, same timing
+    cases = None
+    if args.workload.startswith("loguniform_f64_2p28_") and not args.no_cases:
+        cases = {}
+        for cb, cE in F64_2P28_CASES:
+            key = f"b{cb}_e{cE}"
+            if (cb, cE) == (bits, E):
+                c_ms, d_ms, viol = comp_avg, decomp_avg, errors["bound_violations"]
+            else:
+                c_ms, d_ms, viol = time_case(x, y, cb, cE, args.warmup, K, stream)
+            nb = algorithmic_bytes(dtype, n, cb, cE)
+            cases[key] = {"compress_gbs": round(nb / c_ms / 1e6, 1), "decompress_gbs": round(nb / d_ms / 1e6, 1),
+                          "compress_frac": round(nb / c_ms / 1e6 / peaks["hbm_gbs"], 4),
+                          "decompress_frac": round(nb / d_ms / 1e6 / peaks["hbm_gbs"], 4),
+                          "algorithmic_bytes": nb, "bound_violations": viol}
 
     # ---- end to end through the host-buffer C ABI
     e2e = None
@@ -433,12 +481,12 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
     # ---- CPU baseline: reference codec on the host cores, rank 0 at N = 1
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        sample = min(n, 1 << 24)
-        xs = x[:sample].cpu().numpy()
+        xs = x.cpu().numpy()
         threads = os.cpu_count() or 1
         gbs, ckind, reps = cpu_reference_codec(xs, bits, E, threads, args.cpu_seconds)
         cpu = {"value": round(gbs, 3), "unit": "GB/s", "cores": threads, "kind": ckind,
-               "sample": f"first {sample} values of the workload, compress+decompress, {reps} reps"}
+               "sample": f"all {n} values of the workload, compress+decompress, {reps} reps"}
+        del xs
 
     if dist:
         dist.barrier()
@@ -446,7 +494,6 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
     if rank != 0:
         return
 
-    peaks = load_peaks()
     dom_ms = max(comp_avg, decomp_avg)
     dom = "compress" if comp_avg >= decomp_avg else "decompress"
     achieved = per_launch / (dom_ms / 1e3) / 1e9
@@ -470,6 +517,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
                      "unit": "GB/s", "frac": round(achieved / peaks["hbm_gbs"], 4), "traffic": traffic,
                      "algorithmic_bytes": per_launch, "peak_source": peaks["source"]},
         "errors": errors,
+        **({"cases": {"of": f"measured HBM copy {peaks['hbm_gbs']} GB/s", "steps": K, **cases}} if cases else {}),
         "cpu_baseline": cpu,
         "e2e": e2e,
         "gpu_launches": 2 * K,
@@ -850,6 +898,8 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=3.0)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-cases", action="store_true",
+                    help="2 GiB fp64 workloads: skip timing the configuration's other five cases")
     ap.add_argument("--requests", type=int, default=100_000, help="serving: requests in the Poisson stream")
     ap.add_argument("--capacity-requests", type=int, default=20_000, help="serving: requests of the capacity probe")
     ap.add_argument("--load", type=float, default=0.7, help="serving: offered load as a fraction of capacity")

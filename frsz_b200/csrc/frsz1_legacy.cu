@@ -38,16 +38,22 @@ constexpr int kLegacyBlock = 256; // src/frsz.cc:103, 132
 
 // std::round (half away from zero) of a double with additions only, by the
 // magic-constant method for rounding to an integer (Muller et al., Handbook
-// of Floating-Point Arithmetic, 2nd ed., sec. 5.1): for |p| < 2^52, |p| + 0.5
-// is exact, and adding 2^52 rounded toward zero leaves floor(|p| + 0.5) +
-// 2^52, from which 2^52 is subtracted exactly; the sign is copied back (so
-// -0.4 gives -0.0 as std::round does).  |p| >= 2^52 (already an integer),
-// Inf and NaN are returned as they are.
+// of Floating-Point Arithmetic, 2nd ed., sec. 5.1): adding 2^52 rounded
+// toward zero to v = |p| + 0.5 leaves floor(v) + 2^52, from which 2^52 is
+// subtracted exactly.  v itself is rounded, but for 0.5 <= |p| < 2^52 that
+// rounding never carries it across an integer: |p| and 0.5 are multiples of
+// ulp(|p|), so v is exact unless it has moved into the next binade, and a
+// binade starts at a power of two, which is an integer with no other integer
+// within 0.5 above it.  Below 0.5 it can: |p| = 0.5 - 2^-54 (the double just
+// below 0.5) gives v = 1 - 2^-54, which rounds to 1.0, where std::round gives
+// 0.  So |p| < 0.5 is 0 by a select.  The sign is copied back (so -0.4 gives
+// -0.0 as std::round does).  |p| >= 2^52 (already an integer), Inf and NaN
+// are returned as they are.
 __device__ __forceinline__ double round_half_away(double p)
 {
   constexpr double TWO52 = 4503599627370496.0;
   const double a = fabs(p);
-  const double t = __dsub_rn(__dadd_rz(__dadd_rn(a, 0.5), TWO52), TWO52);
+  const double t = a < 0.5 ? 0.0 : __dsub_rn(__dadd_rz(__dadd_rn(a, 0.5), TWO52), TWO52);
   return copysign(a < TWO52 ? t : a, p);
 }
 

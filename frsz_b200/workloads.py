@@ -41,6 +41,28 @@ def loguniform_np(n: int, dtype=np.float64, seed: int = 42, lo: float = -30.0, h
     return x
 
 
+def loguniform_host(n: int, dtype=np.float64, seed: int = 42, chunk: int = 1 << 22, threads: int = 0,
+                    **kw) -> np.ndarray:
+    """loguniform_np's distribution for large n, generated on the host in
+    chunks of `chunk` values, chunk c from its own generator seeded with
+    (seed, c), on `threads` threads (0: all host cores).  The values depend
+    only on (n, dtype, seed, chunk), not on the thread count, so a GPU run
+    and a CPU run that both call this get the same array."""
+    import os
+    from concurrent.futures import ThreadPoolExecutor
+
+    out = np.empty(n, dtype=dtype)
+
+    def fill(c):
+        s = c * chunk
+        m = min(chunk, n - s)
+        out[s:s + m] = loguniform_np(m, dtype, seed=[seed, c], **kw)
+
+    with ThreadPoolExecutor(max_workers=threads or os.cpu_count() or 1) as ex:
+        list(ex.map(fill, range(-(-n // chunk))))
+    return out
+
+
 def uniform_np(n: int, lo: float, hi: float, dtype=np.float32, seed: int = 42) -> np.ndarray:
     return np.random.default_rng(seed).uniform(lo, hi, n).astype(dtype)
 

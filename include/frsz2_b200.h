@@ -179,8 +179,11 @@ void frsz2_batch_destroy(frsz2_batch* plan);
  * device array of the library (4096 arrays at most per call; larger calls
  * return 2), held by every GPU that loads the library until exit, shared by
  * all calls: calls whose work overlaps on the GPU (other streams or threads)
- * race.  The first call on each device sets the array up; make it before any
- * stream capture. */
+ * race; calls on one stream are ordered.  The descriptors reach the array
+ * through kernel parameters, so no host copy is kept between calls.  The first
+ * call on each device sets the array up (looks up its device address, which
+ * is kept for the process); make it before any stream capture.  Calls after
+ * cudaDeviceReset on that device are not supported. */
 int frsz2_batch_compress_static(const frsz2_batch_item* items, uint64_t count, void* stream);
 
 /* ---------------------------------------------------------------------------

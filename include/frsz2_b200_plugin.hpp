@@ -15,8 +15,9 @@
 // the reference's output_size() (src/frsz2.cc:136-150) computes a smaller,
 // legacy size and the codec then writes past the end of that buffer.
 //
-// INTEGRATION.md shows the LibPressio subclass a maintainer would derive
-// from this class when LibPressio is available.
+// Where LibPressio is available, a maintainer derives the LibPressio
+// compressor plugin from this class: its options, configuration and
+// documentation map one to one onto LibPressio's pressio_options entries.
 #ifndef FRSZ2_B200_PLUGIN_HPP
 #define FRSZ2_B200_PLUGIN_HPP
 

@@ -33,11 +33,17 @@ _c_size = ctypes.c_size_t
 _vp = ctypes.c_void_p
 
 
+def reference_dir() -> str:
+    """The reference checkout: $FRSZ_REF_DIR, else a `reference` directory
+    beside the repository (the Makefile's rule)."""
+    return os.environ.get("FRSZ_REF_DIR") or os.path.abspath(os.path.join(HERE, os.pardir, os.pardir, "reference"))
+
+
 def build(with_reference: bool = True) -> None:
     """Compile the restatement (and, where the reference sources exist, the
     reference shim).  Uses the committed Makefile."""
     target = "all" if with_reference else os.path.join(HERE, "libfrsz2_oracle.so")
-    subprocess.run(["make", "-s", "-C", HERE, target], check=True)
+    subprocess.run(["make", "-s", "-C", HERE, f"REF_DIR={reference_dir()}", target], check=True)
 
 
 def _np_ptr(a: np.ndarray):

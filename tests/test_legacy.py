@@ -38,6 +38,145 @@ def test_oracle_block_rules():
     assert y_ref[256] == x[256] and y_ref[257] == x[256] + 2.0
 
 
+# ------------------------------------------------------------------ known answers
+# Each case below is worked out by hand from the reference's lines: the
+# quantizer quantized[i] = std::round(data[i] * ebx2_inv) (src/frsz.cc:125,
+# half away from zero, in double), the difference within blocks of 256
+# (:128-129) and saturate<int16_t> (:99-103); the decoder's per-block loop
+# `for block_idx < (len/BLOCK)+1` with `if (BLOCK*block_idx < len)` and its
+# running sum over quantized[i], i the index within the block (:140-151).
+
+HALF = np.nextafter(0.5, 0.0)  # 0.49999999999999994
+
+
+def fp32_eps_for(p_target: float, seed_x: float):
+    """A float x and an epsilon for which (double) x * (1 / (2 eps)) is
+    exactly p_target: searched over floats x near seed_x and, for each, the
+    doubles next to x / (2 p_target)."""
+    xf = np.float32(seed_x)
+    for _ in range(64):
+        e0 = float(xf) / (2.0 * p_target)
+        for d in range(-64, 65):
+            e = e0
+            step = np.inf if d > 0 else -np.inf
+            for _ in range(abs(d)):
+                e = np.nextafter(e, step)
+            if float(xf) * (1.0 / (e * 2.0)) == p_target:
+                return xf, float(e)
+        xf = np.nextafter(xf, np.float32(np.inf))
+    raise AssertionError(f"no float and epsilon give {p_target!r}")
+
+
+def rounding_known_answers():
+    """(dtype, x, epsilon, expected int16 stream)."""
+    out = [
+        # epsilon 0.5: step 1, p = x.  Ties go away from zero (2.5 -> 3, not 2);
+        # the double below 0.5 rounds to 0; one ulp either side of 2.5 gives 2
+        # and 3; -HALF gives -0.  Differences: 1-0, 2-1, 3-2, -1-3, -3+1, 0+3,
+        # 2-0, 3-2, -0-3.
+        (np.float64, [0.5, 1.5, 2.5, -0.5, -2.5, HALF, np.nextafter(2.5, 0), np.nextafter(2.5, 9), -HALF], 0.5,
+         [1, 1, 1, -4, -2, 3, 2, 1, -3]),
+        # a float input whose p is the double just below 0.5: q = 0
+        (np.float32, [3.202960252761841], 3.2029602527618413, [0]),
+    ]
+    # float inputs with p one double-ulp either side of k + 0.5: q = k, then k + 1
+    for k in (0, 1, 2, 7, 100, 4095):
+        xl, lo = fp32_eps_for(np.nextafter(k + 0.5, 0.0), 2 * k + 1.37)
+        xh, hi = fp32_eps_for(np.nextafter(k + 0.5, np.inf), 2 * k + 1.37)
+        out.append((np.float32, [xl], lo, [k]))
+        out.append((np.float32, [xh], hi, [k + 1]))
+        out.append((np.float32, [-xh], hi, [-(k + 1)]))
+    return out
+
+
+def saturation_known_answers():
+    return [
+        # epsilon 0.5: q = x.  Differences 32767, 32768 (-> 32767), -32768
+        # (exact, not saturated), -32768, 40001 (-> 32767), -80000 (-> -32768),
+        # 40000 (-> 32767)
+        (np.float64, [32767, 65535, 32767, -1, 40000, -40000, 0], 0.5,
+         [32767, 32767, -32768, -32768, 32767, -32768, 32767]),
+        (np.float32, [32767, 65535, 32767, -1, 40000, -40000, 0], 0.5,
+         [32767, 32767, -32768, -32768, 32767, -32768, 32767]),
+        # +-Inf: differences +Inf, -Inf, +Inf, Inf - Inf = NaN (0, the value
+        # x86 code gives the undefined conversion), -Inf, +Inf
+        (np.float32, [np.inf, 0, np.inf, np.inf, -np.inf, 5], 0.5, [32767, -32768, 32767, 0, -32768, 32767]),
+        (np.float64, [np.inf, 0, np.inf, np.inf, -np.inf, 5], 0.5, [32767, -32768, 32767, 0, -32768, 32767]),
+    ]
+
+
+def block_restart_known_answer():
+    # the difference restarts at i = 256: 30000 - 0, not 30000 - 30000
+    x = np.full(258, 30000.0)
+    want = np.zeros(258, dtype=np.int16)
+    want[0] = want[256] = 30000
+    return x, want
+
+
+def decode_streams():
+    """(n, int16 stream, expected values with the reference's decode, with
+    each block's own differences); epsilon 0.5, so 2 eps = 1.  Block 0 holds
+    [0, 1, 1, ...]; block 1 starts at 100 and holds 2s; block 2 starts at -7
+    and holds 5s.  The reference adds block 0's differences (1) in every
+    block: block 1 decodes as 100 + i, block 2 as -7 + i; its own 2s and 5s
+    give 100 + 2i and -7 + 5i.  n = 512 is a multiple of 256, where the
+    (len/BLOCK)+1-th block is empty; n = 257 leaves block 1 one value."""
+    out = []
+    for n in (257, 512, 600):
+        q = np.ones(n, dtype=np.int16)
+        q[0] = 0
+        q[256:512] = 2
+        q[256] = 100
+        if n > 512:
+            q[512:] = 5
+            q[512] = -7
+        ref = np.empty(n)
+        own = np.empty(n)
+        for i in range(n):
+            b, j = divmod(i, 256)
+            ref[i] = j if b == 0 else (100 + j if b == 1 else -7 + j)
+            own[i] = j if b == 0 else (100 + 2 * j if b == 1 else -7 + 5 * j)
+        out.append((n, q, ref, own))
+    return out
+
+
+@pytest.mark.parametrize("dtype,x,eps,want", rounding_known_answers() + saturation_known_answers())
+def test_oracle_quantizer_known_answers(dtype, x, eps, want):
+    with np.errstate(invalid="ignore"):
+        got = oracle.frsz1_compress(np.array(x, dtype=dtype), eps)
+    assert got.tolist() == want
+
+
+def test_oracle_block_restart_and_decode_known_answers():
+    x, want = block_restart_known_answer()
+    for dtype in (np.float32, np.float64):
+        assert np.array_equal(oracle.frsz1_compress(x.astype(dtype), 0.5), want)
+    for n, q, ref, own in decode_streams():
+        for dtype in (np.float32, np.float64):
+            assert np.array_equal(oracle.frsz1_decompress(q, dtype, 0.5), ref.astype(dtype)), n
+            assert np.array_equal(oracle.frsz1_decompress(q, dtype, 0.5, own_deltas=True), own.astype(dtype)), n
+
+
+@pytest.mark.gpu
+def test_gpu_known_answers(cuda):
+    """The kernels give the hand-derived answers above, bit for bit; decoding
+    writes nothing past n (canary slack)."""
+    for dtype, x, eps, want in rounding_known_answers() + saturation_known_answers():
+        t = torch.from_numpy(np.array(x, dtype=dtype)).cuda()
+        assert legacy.compress(t, eps).cpu().tolist() == want, (dtype, x, eps)
+    x, want = block_restart_known_answer()
+    for dtype in (np.float32, np.float64):
+        assert np.array_equal(legacy.compress(torch.from_numpy(x.astype(dtype)).cuda(), 0.5).cpu().numpy(), want)
+    for n, q, ref, own in decode_streams():
+        for dtype, tdt in ((np.float32, torch.float32), (np.float64, torch.float64)):
+            for own_deltas, expect in ((False, ref), (True, own)):
+                out = torch.full((n + 64,), -3.0, dtype=tdt, device="cuda")
+                legacy.decompress(torch.from_numpy(q).cuda(), tdt, 0.5, own_deltas=own_deltas, out=out[:n])
+                got = out.cpu().numpy()
+                assert np.array_equal(got[:n], expect.astype(dtype)), (n, dtype, own_deltas)
+                assert np.all(got[n:] == -3.0), (n, dtype, own_deltas)
+
+
 def test_plugin_surface():
     # src/frsz.cc:19-46, 82-86, 160; CMakeLists.txt:3 (project version)
     p = legacy.Frsz1Plugin()
