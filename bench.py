@@ -526,6 +526,110 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
     print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------------- one array over several GPUs
+
+def run_shard(args, rank: int, world: int, local_rank: int) -> None:
+    """One array split across the ranks by block range (strong scaling): rank
+    r compresses and decompresses only its blocks, writing them into the
+    whole array's layout (frsz2_compress_blocks / frsz2_decompress_blocks);
+    there is no data-path collective.  value = the whole array's algorithmic
+    bytes per step over the slowest rank's time."""
+    import torch
+
+    import frsz_b200
+    from frsz_b200 import shard
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local_rank))
+    kind, dtype, n, bits, E = WORKLOADS[args.workload][:5]
+    frsz_b200.lib()
+    x_full = make_input_cuda(kind, dtype, n, args.seed)  # the same array on every rank
+    b0, b1 = shard.shard_blocks(n, dtype, bits, E, world, rank)
+    v0, v1 = b0 * E, min(n, b1 * E)
+    xs = x_full[v0:v1].clone()
+    ys = torch.empty_like(xs)
+    buf = torch.zeros(frsz_b200.compressed_size(dtype, bits, E, n), dtype=torch.uint8, device="cuda")
+    stream = torch.cuda.current_stream()
+    mine = algorithmic_bytes(dtype, v1 - v0, bits, E) if v1 > v0 else 0
+
+    def step(ev=None):
+        if ev is not None:
+            ev[0].record(stream)
+        if v1 > v0:
+            shard.compress_shard(xs, n, bits, E, b0, b1, buf, stream=stream)
+        if ev is not None:
+            ev[1].record(stream)
+        if v1 > v0:
+            shard.decompress_shard(buf, n, dtype, bits, E, b0, b1, ys, stream=stream)
+        if ev is not None:
+            ev[2].record(stream)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    K = args.steps
+    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(K)]
+    clocks = ClockSampler(torch.cuda.current_device()) if rank == 0 else None
+    if clocks:
+        clocks.start()
+        time.sleep(0.3)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    for k in range(K):
+        step(evs[k])
+    t1.record(stream)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clk = clocks.stop() if clocks else None
+    elapsed_ms = t0.elapsed_time(t1)
+    comp_avg = statistics.mean(e[0].elapsed_time(e[1]) for e in evs)
+    decomp_avg = statistics.mean(e[1].elapsed_time(e[2]) for e in evs)
+    # this rank's bytes equal a whole-array compress over its written ranges
+    whole = frsz_b200.compress(x_full, bits, E)
+    ok = all(torch.equal(buf[o:o + ln], whole[o:o + ln]) for o, ln in shard.written_ranges(n, bits, E, b0, b1))
+    del whole
+    if dist:
+        t = torch.tensor([elapsed_ms, comp_avg, decomp_avg, 0.0 if ok else 1.0], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        elapsed_ms, comp_avg, decomp_avg, bad = (float(v) for v in t)
+        ok = bad == 0.0
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    assert ok, "a shard's bytes differ from the whole-array compress"
+    peaks = load_peaks()
+    per_launch = algorithmic_bytes(dtype, n, bits, E)
+    dom_ms = max(comp_avg, decomp_avg)
+    achieved = mine / (dom_ms / 1e3) / 1e9
+    line = {
+        "metric": METRIC, "value": round(2 * per_launch * K / (elapsed_ms / 1e3) / 1e9, 3), "unit": "GB/s",
+        "n_gpus": world, "steps": K, "warmup": args.warmup, "ms_per_step": round(elapsed_ms / K, 5),
+        "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+        "dtype": "u32" if dtype == "float32" else "u64", "data": "synthetic",
+        "config": {"workload": args.workload, "dtype": dtype, "n": n, "bits": bits, "block_size": E,
+                   "bytes_per_step": 2 * per_launch, "l2": "inputs larger than L2, no flush",
+                   "parallelism": f"block-range shards x{world}", "rank0_blocks": [b0, b1]},
+        "roofline": {"bound": "hbm", "kernel": "compress" if comp_avg >= decomp_avg else "decompress",
+                     "achieved": round(achieved, 2), "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                     "frac": round(achieved / peaks["hbm_gbs"], 4), "traffic": None,
+                     "algorithmic_bytes": mine, "peak_source": peaks["source"], "of": "rank 0's shard"},
+        "cpu_baseline": None, "e2e": None, "gpu_launches": 2 * K, "clocks": clk,
+    }
+    print(json.dumps(line), flush=True)
+
+
 # ---------------------------------------------------------------- batched
 
 def batched_specs(count: int = 4096, seed: int = 7):
@@ -908,6 +1012,9 @@ def main():
                     help="batched4096: keep the plan's default launch shape")
     ap.add_argument("--krylov-vectors", type=int, default=100, help="krylov100: basis size")
     ap.add_argument("--streams", type=int, default=4)
+    ap.add_argument("--shard", action="store_true",
+                    help="split one array across the ranks by block range (strong scaling) instead of one "
+                         "array per rank")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     rank = int(os.environ.get("RANK", "0"))
@@ -923,6 +1030,8 @@ def main():
         run_legacy(args, rank, world, local_rank)
     elif args.impl == "reference":
         run_reference_arm(args, rank, world)
+    elif args.shard:
+        run_shard(args, rank, world, local_rank)
     else:
         run_ours(args, rank, world, local_rank)
 

@@ -1,0 +1,5 @@
+// fp64 instances of the compile-time block-size kernels
+// (frsz2_blockwise_ce.cuh) for blocks of 12 values, bits 4..64.
+#include "frsz2_blockwise_ce.cuh"
+
+FRSZ2_BWC_DEFINE(f64, double, 12, 4, 61)

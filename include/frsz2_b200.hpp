@@ -17,6 +17,14 @@
 //       decompress_gpu_element (device code)     -- random access inside the
 //           caller's own kernels (include/frsz2.hpp:1096-1104); compiled
 //           when the including file is built by nvcc
+//   frsz::compress_gpu<Comp, block_size> / frsz::decompress_gpu<Comp>
+//     (include/frsz2.hpp:1258-1288) -- the reference's launchable kernels,
+//     same names, template and kernel parameters, any launch shape (the
+//     reference tests launch <<<ceil(n / 4E), 4E>>> and
+//     <<<ceil(n / (max(1, 512/E) E)), max(1, 512/E) E>>>), so code that
+//     launches them compiles and produces the same bytes; nvcc only.  They
+//     run simple one-thread-per-block / per-value device code; the
+//     library's compress_gpu_impl / decompress_gpu_impl are the fast path.
 //   frsz::int_list_t, frsz::dispatch_frsz2_compression /
 //   dispatch_frsz2_decompression  (include/frsz2.hpp:1292-1347)
 //     same signatures and std::runtime_error messages; host buffers.
@@ -38,6 +46,9 @@
 
 #if defined(__CUDACC__)
 #include "frsz2_b200_device.cuh"
+#define FRSZ2_B200_HD __host__ __device__
+#else
+#define FRSZ2_B200_HD
 #endif
 
 namespace frsz {
@@ -90,6 +101,10 @@ struct frsz2_compressor
   static_assert(0 < max_exp_block_size, "max_exp_block_size must be positive!");
   static_assert(4 <= bits_per_value, "Minimum bits per value is 4 (so at most 2 values share the same byte).");
   static_assert(bits_per_value <= 64, "maximum number for bits_per_value is 64.");
+  // A narrowing of the reference, which only asks for 0 < E: the library's
+  // kernels index bits within one block with 32-bit integers, so blocks are
+  // capped at 65536 values (65536 * 64 bits < 2^31); the C ABI rejects larger
+  // ones with status 2.
   static_assert(max_exp_block_size <= 65536, "this library supports exponent blocks of up to 65536 values");
 
   static constexpr int uint_compressed_size_bit = sizeof(uint_compressed_type) * CHAR_BIT;
@@ -120,13 +135,13 @@ struct frsz2_compressor
   {
   }
 
-  uint_compressed_type* get_compressed_data() { return compressed_; }
-  const uint_compressed_type* get_compressed_data() const { return compressed_; }
-  const uint_compressed_type* get_const_compressed_data() const { return compressed_; }
-  exp_type* get_exponent_data() { return exponents_; }
-  const exp_type* get_exponent_data() const { return exponents_; }
-  const exp_type* get_const_exponent_data() const { return exponents_; }
-  std::size_t get_total_elements() const { return total_elements_; }
+  FRSZ2_B200_HD uint_compressed_type* get_compressed_data() { return compressed_; }
+  FRSZ2_B200_HD const uint_compressed_type* get_compressed_data() const { return compressed_; }
+  FRSZ2_B200_HD const uint_compressed_type* get_const_compressed_data() const { return compressed_; }
+  FRSZ2_B200_HD exp_type* get_exponent_data() { return exponents_; }
+  FRSZ2_B200_HD const exp_type* get_exponent_data() const { return exponents_; }
+  FRSZ2_B200_HD const exp_type* get_const_exponent_data() const { return exponents_; }
+  FRSZ2_B200_HD std::size_t get_total_elements() const { return total_elements_; }
 
   // Host buffers (the view's buffer and `data` in host memory).
   int compress_cpu_impl(const fp_type* data)
@@ -188,6 +203,17 @@ struct frsz2_compressor
     return frsz2_b200::device::decode_element<bits_per_value, max_exp_block_size, fp_type>(exponents_, compressed_,
                                                                                          idx);
   }
+  // Compress exponent block `block` of the array `data` (device memory, all
+  // get_total_elements() values) into the view's buffer: its exponent and
+  // the words its values reach, the bytes compress_cpu_impl writes.
+  __device__ void compress_gpu_block(std::size_t block, const fp_type* data)
+  {
+    const std::size_t first = block * (std::size_t)max_exp_block_size;
+    const std::size_t left = total_elements_ - first;
+    const std::size_t cnt = left < (std::size_t)max_exp_block_size ? left : (std::size_t)max_exp_block_size;
+    frsz2_b200::device::encode_block<bits_per_value, max_exp_block_size, fp_type>(data + first, cnt, exponents_,
+                                                                                compressed_, block);
+  }
 #endif
 
 private:
@@ -196,6 +222,34 @@ private:
   uint_compressed_type* const compressed_;
   const std::size_t total_elements_;
 };
+
+#if defined(__CUDACC__)
+// The reference's launchable kernels (include/frsz2.hpp:1258-1288), same
+// names and parameters.  Any grid works: compress_gpu's threads take whole
+// exponent blocks in a grid-stride loop (the reference's launch of one thread
+// per value leaves the threads past the block count idle), decompress_gpu's
+// threads take values as the reference's do.  The bytes written equal
+// compress_cpu_impl's and the values decompress_cpu_impl's, bit for bit.
+template<typename Frsz2Compressor, int block_size>
+__global__ __launch_bounds__(block_size) void compress_gpu(const typename Frsz2Compressor::fp_type* __restrict__ data,
+                                                           Frsz2Compressor compressor)
+{
+  constexpr std::size_t E = (std::size_t)Frsz2Compressor::max_exp_block_size;
+  const std::size_t nb = (compressor.get_total_elements() + E - 1) / E;
+  for (std::size_t b = (std::size_t)blockIdx.x * blockDim.x + threadIdx.x; b < nb;
+       b += (std::size_t)gridDim.x * blockDim.x)
+    compressor.compress_gpu_block(b, data);
+}
+
+template<typename Frsz2Compressor>
+__global__ void decompress_gpu(typename Frsz2Compressor::fp_type* const __restrict__ output,
+                               Frsz2Compressor compressor)
+{
+  for (std::size_t idx = (std::size_t)blockIdx.x * blockDim.x + threadIdx.x; idx < compressor.get_total_elements();
+       idx += (std::size_t)gridDim.x * blockDim.x)
+    output[idx] = compressor.decompress_gpu_element(idx);
+}
+#endif
 
 // ---------------------------------------------------------------- dispatch
 // include/frsz2.hpp:1292-1347: recursive walk from runtime (bits, E) to a
@@ -279,5 +333,7 @@ void dispatch_frsz2_decompression(int_list_t<bit_values...> bl, int actual_bits_
 }
 
 } // namespace frsz
+
+#undef FRSZ2_B200_HD
 
 #endif // FRSZ2_B200_HPP

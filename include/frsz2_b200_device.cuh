@@ -107,6 +107,97 @@ __device__ __forceinline__ T decode_element(const void* exponents, const void* w
   return decode_code<T, BITS>((typename ieee<T>::U)c, be);
 }
 
+// ---------------------------------------------------------------- encode
+
+// Unbiased exponent of x from its bit field, narrowed to the reference's
+// exponent_t (int8 for float, so the Inf/NaN field gives -128; int16 for
+// double); zero and subnormals give -bias (include/frsz2.hpp:312-320).
+template<class T>
+__device__ __forceinline__ int exponent_of(T x)
+{
+  using F = ieee<T>;
+  typename F::U u;
+  if constexpr (sizeof(T) == 4)
+    u = __float_as_uint(x);
+  else
+    u = (std::uint64_t)__double_as_longlong(x);
+  const int field = (int)((u >> F::SIG) & ((1u << F::EXPB) - 1));
+  if constexpr (sizeof(T) == 4)
+    return (int)(std::int8_t)(field - F::BIAS);
+  else
+    return (int)(std::int16_t)(field - F::BIAS);
+}
+
+// The `bits`-wide code of x in a block with exponent be: the sign-magnitude
+// fixed-point value of x with the block maximum's leading bit at the top
+// magnitude position (include/frsz2.hpp:352-376: significand with its
+// implicit bit unless the exponent is -bias, shifted by (exponent bits - 1)
+// - (be - e), truncated, no rounding; shifts that leave the word give 0),
+// cut to its top `bits` bits (include/frsz2.hpp:555-558).
+template<class T, int BITS>
+__device__ __forceinline__ typename ieee<T>::U encode_value(T x, std::int16_t be)
+{
+  using F = ieee<T>;
+  using U = typename F::U;
+  U u;
+  if constexpr (sizeof(T) == 4)
+    u = __float_as_uint(x);
+  else
+    u = (std::uint64_t)__double_as_longlong(x);
+  const int e = exponent_of(x);
+  U m = u & ((U(1) << F::SIG) - 1);
+  if (e != -F::BIAS) m |= U(1) << F::SIG;
+  const int shift = F::EXPB - 1 - ((int)be - e);
+  U r;
+  if (shift < -F::SIG)
+    r = 0;
+  else if (shift > 0)
+    r = shift >= F::UBITS ? U(0) : (U)(m << shift);
+  else
+    r = m >> (-shift);
+  r |= u & (U(1) << (F::UBITS - 1));
+  return r >> (F::UBITS - BITS);
+}
+
+// Compress exponent block b of an array into its exponent and its words
+// (the layout of include/frsz2.hpp:525-548): x points at the block's first
+// value and cnt (1..E) is its count.  The block exponent is the exponent of
+// the largest magnitude, NaNs skipped as std::max skips them
+// (include/frsz2.hpp:1121-1125), stored as the signed word-width exponent;
+// codes are packed LSB-first (include/frsz2.hpp:565-644), and only the words
+// the cnt values reach are written, as compress_cpu_block writes them
+// (include/frsz2.hpp:1108-1179).
+template<int BITS, int E, class T>
+__device__ inline void encode_block(const T* x, std::size_t cnt, void* exponents, void* words, std::size_t b)
+{
+  using Word = std::conditional_t<
+    (BITS <= 8), std::uint8_t,
+    std::conditional_t<(BITS <= 16), std::uint16_t, std::conditional_t<(BITS <= 32), std::uint32_t, std::uint64_t>>>;
+  using Exp = std::make_signed_t<Word>;
+  constexpr int W = (int)sizeof(Word) * 8;
+  constexpr std::size_t BLOCK_WORDS = ((std::size_t)E * BITS + W - 1) / W;
+  T in_max = 0;
+  for (std::size_t k = 0; k < cnt; ++k) {
+    const T a = x[k] < T(0) ? -x[k] : x[k]; // a NaN stays a NaN
+    in_max = in_max < a ? a : in_max;       // false for a NaN: skipped
+  }
+  const Exp be = (Exp)exponent_of(in_max);
+  static_cast<Exp*>(exponents)[b] = be;
+  Word* wb = static_cast<Word*>(words) + b * BLOCK_WORDS;
+  Word cur = 0;
+  std::size_t w = 0;
+  for (std::size_t k = 0; k < cnt; ++k) {
+    const std::uint64_t c = (std::uint64_t)encode_value<T, BITS>(x[k], (std::int16_t)be);
+    const int o = (int)((k * BITS) % W);
+    cur |= (Word)(c << o);
+    if (o + BITS >= W) { // word w is complete
+      wb[w++] = cur;
+      cur = o + BITS > W ? (Word)(c >> (W - o)) : Word(0);
+    }
+  }
+  if ((cnt * BITS) % W != 0) wb[w] = cur; // the partly filled last word
+}
+
 } // namespace device
 } // namespace frsz2_b200
 

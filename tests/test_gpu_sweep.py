@@ -214,3 +214,44 @@ def test_pointers_off_alignment(cuda, dtype, bits, E):
         want = oracle.decompress(ref, n, dtype, bits, E)
         uint = np.uint64 if dtype == np.float64 else np.uint32
         assert np.array_equal(y[voff:voff + n].cpu().numpy().view(uint), want.view(uint)), (voff, boff)
+
+
+@pytest.mark.parametrize("dtype,bits", [(np.float32, b) for b in range(4, 33)] + [(np.float64, b) for b in range(4, 65)])
+def test_compile_time_block_sizes_every_width(cuda, dtype, bits):
+    """Block sizes 6, 7 and 12, which have compile-time instances (as 3 and
+    5 do, above): every width, several chunks of whole blocks, a partial
+    last block, special values."""
+    es = np.dtype(dtype).itemsize
+    for E in (6, 7, 12):
+        n = (5 * 4096 if es == 4 else 5 * 2048) + 3 * E + E // 2 + 1
+        check(special_values(dtype, n, bits * 17 + E), bits, E)
+
+
+@pytest.mark.parametrize("E", [3, 5, 6, 7, 12])
+def test_compile_time_block_sizes_off_alignment(cuda, E):
+    """Values and buffers off 16-byte boundaries on the compile-time block
+    sizes: bytes and values equal the oracle's, nothing written outside."""
+    for dtype, bits in ((np.float32, 9), (np.float32, 16), (np.float32, 21), (np.float64, 9), (np.float64, 33)):
+        es = np.dtype(dtype).itemsize
+        n = 3 * 4096 + 2 * E + 1
+        x = special_values(dtype, n, bits + E)
+        size = frsz_b200.compressed_size(dtype, bits, E, n)
+        w = frsz_b200.word_bits(bits) // 8
+        tdt = torch.float32 if es == 4 else torch.float64
+        uint = np.uint32 if es == 4 else np.uint64
+        for voff, boff in ((1, w), (3, 3 * w)):
+            tv = torch.zeros(n + 4, dtype=tdt, device="cuda")
+            tv[voff:voff + n] = torch.from_numpy(x).cuda()
+            raw = torch.full((size + 64,), 0x5A, dtype=torch.uint8, device="cuda")
+            buf = raw[boff:boff + size]
+            frsz_b200.compress(tv[voff:voff + n], bits, E, out=buf)
+            ref = oracle.compress(x, bits, E, canary=0x5A)
+            assert np.array_equal(buf.cpu().numpy(), ref), (dtype, bits, voff, boff)
+            r = raw.cpu().numpy()
+            assert np.all(r[:boff] == 0x5A) and np.all(r[boff + size:] == 0x5A)
+            y = torch.full((n + 4,), -7.0, dtype=tdt, device="cuda")
+            frsz_b200.decompress(buf, n, dtype, bits, E, out=y[voff:voff + n])
+            got = y.cpu().numpy()
+            want = oracle.decompress(ref, n, dtype, bits, E)
+            assert np.array_equal(got[voff:voff + n].view(uint), want.view(uint)), (dtype, bits, voff, boff)
+            assert np.all(got[:voff] == -7.0) and np.all(got[voff + n:] == -7.0)
