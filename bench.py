@@ -19,12 +19,15 @@ the same way on the same array, under "cases".
             bandwidth
   cpu_baseline  the reference's own CPU codec (oracle/_ref, all host threads)
             on the same whole array
+  extras    (default workload, one GPU) short runs of the batched (4,096
+            arrays in one persistent launch per class vs per-array calls), fused
+            basis dot / axpy and serving workloads, summarised
 
 ``--impl reference`` times that reference CPU codec alone on the same
 workload (the whole array, the same values) and prints the reference-arm
-line.  Under torchrun every rank
-compresses its own field (weak scaling, no data-path collective); the timing
-is the max over ranks.
+line.  Under torchrun every rank compresses its own array (weak scaling, no
+data-path collective), or with --shard one array split by block range (strong
+scaling); the timing is the max over ranks.
 """
 from __future__ import annotations
 
@@ -494,6 +497,14 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
     if rank != 0:
         return
 
+    # ---- the other north-star measurements, summarised in the same line (N = 1,
+    # default workload): batched, fused basis dot / axpy, serving
+    extras = None
+    if world == 1 and args.extras and args.workload == DEFAULT_WORKLOAD:
+        del x, y, buf
+        torch.cuda.empty_cache()
+        extras = run_extras(args, local_rank)
+
     dom_ms = max(comp_avg, decomp_avg)
     dom = "compress" if comp_avg >= decomp_avg else "decompress"
     achieved = per_launch / (dom_ms / 1e3) / 1e9
@@ -522,8 +533,51 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
         "e2e": e2e,
         "gpu_launches": 2 * K,
         "clocks": clk,
+        **({"extras": extras} if extras else {}),
     }
     print(json.dumps(line), flush=True)
+
+
+def run_extras(args, local_rank: int) -> dict:
+    """Short runs of the batched (4,096 arrays), fused basis dot / axpy and
+    serving workloads, summarised; each is the same code as its own
+    --workload run (plan autotuning skipped, its default shape kept), and a
+    failure is recorded instead of ending the benchmark."""
+    import copy
+
+    import torch
+
+    out = {}
+    for name, fn in (("batched4096", run_batched), ("krylov100", run_krylov), ("serving", run_serving)):
+        a = copy.copy(args)
+        a.batch_autotune = False
+        t0 = time.perf_counter()
+        try:
+            line = fn(a, 0, 1, local_rank, emit=False)
+        except Exception as e:  # recorded, the headline stands
+            out[name] = {"error": repr(e)[:300]}
+            continue
+        finally:
+            torch.cuda.synchronize()
+            torch.cuda.empty_cache()
+        if name == "batched4096":
+            out[name] = {"gbs": line["value"], "hbm_frac": line["batched"]["hbm_frac"],
+                         "compress_gbs": line["batched"]["compress_gbs"],
+                         "decompress_gbs": line["batched"]["decompress_gbs"],
+                         "per_array_plain_gbs": line["per_array_plain"]["gbs"],
+                         "per_array_graph_gbs": line["per_array_graph"]["gbs"],
+                         "speedup_vs_per_array_plain": line["speedup_vs_per_array_plain"],
+                         "speedup_vs_per_array_graph": line["speedup_vs_per_array_graph"],
+                         "bytes_per_step": line["config"]["bytes_per_step"], "steps": line["steps"]}
+        elif name == "krylov100":
+            out[name] = {"fused_dot": line["fused_dot"], "fused_axpy": line["fused_axpy"],
+                         "uncompressed_torch_ms": line["uncompressed_torch"],
+                         "compressed_basis_bytes": line["config"]["compressed_basis_bytes"]}
+        else:
+            out[name] = {"gbs": line["value"], "latency_us": line["latency_us"], "capacity": line["capacity"],
+                         "requests": line["config"]["requests"], "load": line["config"]["load"]}
+        out[name]["wall_s"] = round(time.perf_counter() - t0, 1)
+    return out
 
 
 # ---------------------------------------------------------------- one array over several GPUs
@@ -646,7 +700,7 @@ def batched_specs(count: int = 4096, seed: int = 7):
     return specs
 
 
-def run_batched(args, rank: int, world: int, local_rank: int) -> None:
+def run_batched(args, rank: int, world: int, local_rank: int, emit: bool = True):
     """One step = compress all arrays, then decompress all.  value = the
     batched plan (one graph launch per direction); the same arrays are also
     timed with one plain frsz2_compress / frsz2_decompress call per array
@@ -771,12 +825,14 @@ def run_batched(args, rank: int, world: int, local_rank: int) -> None:
         "speedup_vs_per_array_graph": round(gper_ms / step_ms, 2),
         "gpu_launches": 2 * info["classes"] * K,
     }
-    print(json.dumps(line), flush=True)
+    if emit:
+        print(json.dumps(line), flush=True)
+    return line
 
 
 # ---------------------------------------------------------------- fused basis
 
-def run_krylov(args, rank: int, world: int, local_rank: int) -> None:
+def run_krylov(args, rank: int, world: int, local_rank: int, emit: bool = True):
     """Config 3b: 100 fp64 vectors of 2^22 values, 32 bits, block 32.  Times
     the fused h = V^T w and y += V c over the compressed basis, against
     decompress-then-torch and against torch on the uncompressed basis."""
@@ -854,12 +910,14 @@ def run_krylov(args, rank: int, world: int, local_rank: int) -> None:
         "speedup_fused_axpy_vs_uncompressed": round(ms_dense_axpy / ms_axpy, 2),
         "gpu_launches": 3 * K,  # dot: item kernel + final sum; axpy: one kernel
     }
-    print(json.dumps(line), flush=True)
+    if emit:
+        print(json.dumps(line), flush=True)
+    return line
 
 
 # ---------------------------------------------------------------- serving
 
-def run_serving(args, rank: int, world: int, local_rank: int) -> None:
+def run_serving(args, rank: int, world: int, local_rank: int, emit: bool = True):
     """Config 5: a Poisson stream of requests, 60 % compress / 40 % decompress,
     input sizes log-normal (median 1 MB, sigma 1.5, capped at 256 MB), fp32 /
     fp64 50/50, bits from {12, 16, 32}, block 32, 32 GB admission budget.
@@ -942,7 +1000,9 @@ def run_serving(args, rank: int, world: int, local_rank: int) -> None:
         "offered_requests_per_s": round(lam, 1),
         "server": st,
     }
-    print(json.dumps(line), flush=True)
+    if emit:
+        print(json.dumps(line), flush=True)
+    return line
 
 
 def run_legacy(args, rank: int, world: int, local_rank: int) -> None:
@@ -1002,6 +1062,8 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=3.0)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", dest="extras", action="store_false",
+                    help="default workload: skip the batched / fused basis / serving summaries")
     ap.add_argument("--no-cases", action="store_true",
                     help="2 GiB fp64 workloads: skip timing the configuration's other five cases")
     ap.add_argument("--requests", type=int, default=100_000, help="serving: requests in the Poisson stream")
