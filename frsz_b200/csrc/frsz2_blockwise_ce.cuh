@@ -25,7 +25,19 @@
 
 namespace frsz2b {
 
-template<class T, int BITS, int E>
+#ifndef FRSZ2_BWC_CHUNK_C
+#define FRSZ2_BWC_CHUNK_C 20480
+#endif
+#ifndef FRSZ2_BWC_CHUNK_D
+#define FRSZ2_BWC_CHUNK_D 16384
+#endif
+#ifndef FRSZ2_BWC_QUNROLL
+#define FRSZ2_BWC_QUNROLL 8
+#endif
+// unroll factor of a thread's loop over its blocks in a chunk
+constexpr int kBwcQUnroll = FRSZ2_BWC_QUNROLL;
+
+template<class T, int BITS, int E, bool COMPRESS>
 struct bwc_cfg
 {
   static constexpr int NT = bw_threads<T>();
@@ -33,8 +45,14 @@ struct bwc_cfg
   static constexpr int WB = W / 8;
   static constexpr int NW = (E * BITS + W - 1) / W; // words per block
   static constexpr int BB = NW * WB;                // block bytes
-  static constexpr int BPT0 = bw_bytes<T>() / (NT * E * (int)sizeof(T));
-  static constexpr int BPT = BPT0 < 1 ? 1 : (BPT0 > kBwMaxBpt ? kBwMaxBpt : BPT0); // blocks per thread
+  // values per chunk aimed at: about 20 KB and at most 8 blocks per thread
+  // compressing (the per-chunk work is spread over more blocks than the
+  // run-time-E kernels' 16 KB), 16 KB and at most 4 blocks per thread
+  // decompressing (the next chunk's exponents are held in registers; 5 blocks
+  // per thread at E 3 measured slower)
+  static constexpr int BPT0 = (COMPRESS ? FRSZ2_BWC_CHUNK_C : FRSZ2_BWC_CHUNK_D) / (NT * E * (int)sizeof(T));
+  static constexpr int BPT_MAX = COMPRESS ? 8 : 4;
+  static constexpr int BPT = BPT0 < 1 ? 1 : (BPT0 > BPT_MAX ? BPT_MAX : BPT0); // blocks per thread
   static constexpr int NBC = NT * BPT;               // blocks per chunk
   static constexpr std::uint32_t VAL_BYTES = (std::uint32_t)NBC * E * (std::uint32_t)sizeof(T);
   static constexpr std::uint32_t IMG_BYTES = (std::uint32_t)NBC * BB;
@@ -75,9 +93,51 @@ __device__ __forceinline__ std::int64_t bwc_block_exponent(const typename fp<T>:
   return be;
 }
 
+// encode_plain (the plain-exponent-range code of a value) with one fused
+// multiply-add instead of a multiply and a float-to-integer conversion (a
+// quarter-rate instruction): in the plain range |x| * scale < 2^(BITS-1), so
+// for BITS <= 24 (fp32) or <= 53 (fp64) the exact product plus 2^23 (2^52),
+// rounded toward zero once, is 2^23 + trunc(|x| * scale) -- the magnitude
+// lands in the low bits of the sum (the magic-number method of rounding to an
+// integer, Muller et al., Handbook of Floating-Point Arithmetic, sec. 5.1,
+// here with the rounding toward zero that truncation asks for).  The sign
+// goes in with one bit select: the magnitude's bits above BITS-2 are zero and
+// the shifted bit pattern's bits below BITS-1 are dropped.
+template<class T, int BITS>
+__device__ __forceinline__ typename fast_cfg<T, BITS>::C encode_plain_fma(typename fp<T>::U u, T scale)
+{
+  using C = typename fast_cfg<T, BITS>::C;
+  if constexpr (sizeof(T) == 4) {
+    static_assert(BITS <= 24, "the magnitude must fit below 2^23");
+    const std::uint32_t f = __float_as_uint(__fmaf_rz(fabsf(__uint_as_float(u)), scale, 8388608.0f));
+    constexpr std::uint32_t M = (1u << (BITS - 1)) - 1u;
+    return (f & M) | ((u >> (32 - BITS)) & ~M);
+  } else if constexpr (BITS <= 32) {
+    const double d = __fma_rz(fabs(__longlong_as_double((long long)u)), scale, 4503599627370496.0);
+    const std::uint32_t f = (std::uint32_t)__double2loint(d);
+    constexpr std::uint32_t M = (1u << (BITS - 1)) - 1u;
+    return (f & M) | (((std::uint32_t)(u >> 32) >> (32 - BITS)) & ~M);
+  } else {
+    static_assert(BITS <= 53, "the magnitude must fit below 2^52");
+    const double d = __fma_rz(fabs(__longlong_as_double((long long)u)), scale, 4503599627370496.0);
+    const std::uint64_t f = (std::uint64_t)__double_as_longlong(d);
+    constexpr std::uint64_t M = (1ull << (BITS - 1)) - 1ull;
+    return (C)((f & M) | ((u >> (64 - BITS)) & ~M));
+  }
+}
+
+// Whether encode_plain_fma serves this width.
+template<class T, int BITS>
+constexpr bool fma_encodes()
+{
+  return sizeof(T) == 4 ? BITS <= 24 : BITS <= 53;
+}
+
 // Codes of one block into its W-bit words at dst; a partial block (FULL
 // false) writes only the words its cnt values reach.
-template<class T, int BITS, int E, bool FULL>
+// PLAIN: 1 the block is known to be in the plain range, 0 it is not, -1 test
+// the plain flag.
+template<class T, int BITS, int E, bool FULL, int PLAIN = -1>
 __device__ __forceinline__ void bwc_pack_block(const typename fp<T>::U (&u)[E], int cnt, std::int64_t be, bool plain,
                                                bw_word_t<fast_cfg<T, BITS>::W>* __restrict__ dst)
 {
@@ -108,16 +168,118 @@ __device__ __forceinline__ void bwc_pack_block(const typename fp<T>::U (&u)[E], 
       }
     }
   };
-  if (plain)
-    pack([&](U v) { return encode_plain<T, BITS>(v, scale); });
+  auto plain_code = [&](U v) {
+    if constexpr (fma_encodes<T, BITS>())
+      return encode_plain_fma<T, BITS>(v, scale);
+    else
+      return encode_plain<T, BITS>(v, scale);
+  };
+  if (PLAIN == 1 || (PLAIN == -1 && plain))
+    pack(plain_code);
   else
     pack([&](U v) { return (C)to_code<T>(v, (std::int16_t)be, BITS); });
 }
 
+// Resident CTAs per SM the register budget must allow (0: ptxas's own
+// choice).  Compress is held to 4 (56 registers for fp32 b16 E5; with a
+// bound of 1, ptxas spends 90 on the unrolled blocks, measured 2-8 % slower);
+// decompress keeps ptxas's choice (40 registers there; 72 with a bound of 1,
+// measured slower).
+#ifndef FRSZ2_BWC_MIN_CTAS_C
+#define FRSZ2_BWC_MIN_CTAS_C 4
+#endif
+#ifndef FRSZ2_BWC_MIN_CTAS_D
+#define FRSZ2_BWC_MIN_CTAS_D 0
+#endif
+#if FRSZ2_BWC_MIN_CTAS_C > 0
+#define FRSZ2_BWC_BOUNDS_C(nt) __launch_bounds__(nt, FRSZ2_BWC_MIN_CTAS_C)
+#else
+#define FRSZ2_BWC_BOUNDS_C(nt) __launch_bounds__(nt)
+#endif
+#if FRSZ2_BWC_MIN_CTAS_D > 0
+#define FRSZ2_BWC_BOUNDS_D(nt) __launch_bounds__(nt, FRSZ2_BWC_MIN_CTAS_D)
+#else
+#define FRSZ2_BWC_BOUNDS_D(nt) __launch_bounds__(nt)
+#endif
+
+// One block of cnt (1..E) values at sv, any exponent: block exponent, the
+// per-block choice of plain-range or exact-integer codes, words to dst,
+// exponent to *ep.  Out of line, so the kernels' registers are sized for
+// their inline path (whole warps of plain-range blocks); this one runs for
+// warps holding a block outside the plain range and for the array's last,
+// partial chunk.
 template<class T, int BITS, int E>
-__global__ void __launch_bounds__(bw_threads<T>()) k_compress_bwc(Job j)
+__device__ __noinline__ void bwc_compress_block_any(const typename fp<T>::U* sv, int cnt,
+                                                    bw_word_t<fast_cfg<T, BITS>::W>* dst,
+                                                    bw_word_t<fast_cfg<T, BITS>::W>* ep)
 {
-  using G = bwc_cfg<T, BITS, E>;
+  using U = typename fp<T>::U;
+  using Word = bw_word_t<fast_cfg<T, BITS>::W>;
+  U u[E];
+  bool plain;
+  std::int64_t be;
+  if (cnt == E) {
+#pragma unroll
+    for (int k = 0; k < E; ++k) u[k] = sv[k];
+    be = bwc_block_exponent<T, BITS, E, true>(u, E, plain);
+    bwc_pack_block<T, BITS, E, true>(u, E, be, plain, dst);
+  } else {
+#pragma unroll
+    for (int k = 0; k < E; ++k) u[k] = k < cnt ? sv[k] : U(0);
+    be = bwc_block_exponent<T, BITS, E, false>(u, cnt, plain);
+    bwc_pack_block<T, BITS, E, false>(u, cnt, be, plain, dst);
+  }
+  *ep = (Word)be;
+}
+
+// Chunk staging for a full chunk whose global side starts on a 16-byte
+// boundary (every chunk but an array's last, when the array's pointers are
+// 16-byte aligned): BYTES / 16 whole 16-byte accesses, no head, no tail, the
+// loop bounds and predicates compile-time constants.  The other chunks use
+// bw_issue / bw_commit / chunk_copy.
+template<int NT, int MAXI, std::uint32_t BYTES>
+__device__ __forceinline__ void bwc_issue_full(const std::uint8_t* g, uint4 (&r)[MAXI])
+{
+  constexpr std::uint32_t N16 = BYTES / 16;
+  static_assert(BYTES % 16 == 0 && N16 <= (std::uint32_t)(MAXI * NT), "chunk bytes");
+  const uint4* g16 = reinterpret_cast<const uint4*>(g);
+#pragma unroll
+  for (int i = 0; i < MAXI; ++i) {
+    const std::uint32_t k = threadIdx.x + (std::uint32_t)(i * NT);
+    if (N16 % NT == 0 || k < N16) r[i] = __ldg(g16 + k);
+  }
+}
+
+template<int NT, int MAXI, std::uint32_t BYTES>
+__device__ __forceinline__ void bwc_commit_full(std::uint8_t* s, const uint4 (&r)[MAXI])
+{
+  constexpr std::uint32_t N16 = BYTES / 16;
+  uint4* s16 = reinterpret_cast<uint4*>(s);
+#pragma unroll
+  for (int i = 0; i < MAXI; ++i) {
+    const std::uint32_t k = threadIdx.x + (std::uint32_t)(i * NT);
+    if (N16 % NT == 0 || k < N16) s16[k] = r[i];
+  }
+}
+
+template<int NT, std::uint32_t BYTES>
+__device__ __forceinline__ void bwc_store_full(std::uint8_t* g, const std::uint8_t* s)
+{
+  constexpr std::uint32_t N16 = BYTES / 16;
+  static_assert(BYTES % 16 == 0, "chunk bytes");
+  uint4* g16 = reinterpret_cast<uint4*>(g);
+  const uint4* s16 = reinterpret_cast<const uint4*>(s);
+#pragma unroll
+  for (int i = 0; i < (int)((N16 + NT - 1) / NT); ++i) {
+    const std::uint32_t k = threadIdx.x + (std::uint32_t)(i * NT);
+    if (N16 % NT == 0 || k < N16) __stcs(g16 + k, s16[k]);
+  }
+}
+
+template<class T, int BITS, int E>
+__global__ void FRSZ2_BWC_BOUNDS_C(bw_threads<T>()) k_compress_bwc(Job j)
+{
+  using G = bwc_cfg<T, BITS, E, true>;
   using U = typename fp<T>::U;
   constexpr int NT = G::NT, W = G::W, BB = G::BB, NBC = G::NBC;
   using Word = bw_word_t<W>;
@@ -134,12 +296,20 @@ __global__ void __launch_bounds__(bw_threads<T>()) k_compress_bwc(Job j)
     return reinterpret_cast<const std::uint8_t*>(x + v0);
   };
   uint4 r[G::LOADS_V];
+  // chunk starts are 16-byte multiples apart on both sides (NBC * E values,
+  // NBC * BB bytes), so one test on the array's first chunk covers all
+  static_assert((G::VAL_BYTES % 16) == 0 && (G::IMG_BYTES % 16) == 0, "chunk sizes");
+  const bool aligned = ((reinterpret_cast<std::uintptr_t>(x) | reinterpret_cast<std::uintptr_t>(j.words)) & 15u) == 0;
+  auto issue = [&](std::uint64_t c) {
+    int nvc;
+    const std::uint8_t* g = values_of(c, nvc);
+    if (aligned && nvc == NBC * E)
+      bwc_issue_full<NT, G::LOADS_V, G::VAL_BYTES>(g, r);
+    else
+      bw_issue<NT, G::LOADS_V>(g, (std::uint32_t)nvc * (std::uint32_t)sizeof(T), r);
+  };
   std::uint64_t ch = blockIdx.x;
-  if (ch < nchunks) {
-    int nv0;
-    const std::uint8_t* g0 = values_of(ch, nv0);
-    bw_issue<NT, G::LOADS_V>(g0, (std::uint32_t)nv0 * (std::uint32_t)sizeof(T), r);
-  }
+  if (ch < nchunks) issue(ch);
   for (; ch < nchunks; ch += gridDim.x) {
     const std::uint64_t b0 = ch * (std::uint64_t)NBC;
     int nv;
@@ -148,50 +318,64 @@ __global__ void __launch_bounds__(bw_threads<T>()) k_compress_bwc(Job j)
     std::uint8_t* gout = j.words + b0 * (std::uint64_t)BB;
     const std::uint32_t hv = (std::uint32_t)(reinterpret_cast<std::uintptr_t>(gin) & 15u);
     const std::uint32_t hw = (std::uint32_t)(reinterpret_cast<std::uintptr_t>(gout) & 15u);
-    bw_commit<NT, G::LOADS_V>(gin, s_val, (std::uint32_t)nv * (std::uint32_t)sizeof(T), r);
+    const bool fast = aligned && nv == NBC * E;
+    if (fast)
+      bwc_commit_full<NT, G::LOADS_V, G::VAL_BYTES>(s_val, r);
+    else
+      bw_commit<NT, G::LOADS_V>(gin, s_val, (std::uint32_t)nv * (std::uint32_t)sizeof(T), r);
     __syncthreads();
-    if (ch + gridDim.x < nchunks) { // the next chunk's loads fly while this one is coded
-      int nvn;
-      const std::uint8_t* gn = values_of(ch + gridDim.x, nvn);
-      bw_issue<NT, G::LOADS_V>(gn, (std::uint32_t)nvn * (std::uint32_t)sizeof(T), r);
-    }
+    if (ch + gridDim.x < nchunks) issue(ch + gridDim.x); // the next chunk's loads fly while this one is coded
+    // Every chunk but the array's last is full: its blocks are all whole and
+    // every thread has all its blocks, so that path needs no bounds checks,
+    // and a warp vote sends whole warps down the plain-range encode (a warp
+    // with any block outside that range runs the per-block choice).
+    auto code_blocks = [&](auto full_chunk) {
+      constexpr bool FC = decltype(full_chunk)::value;
+#pragma unroll kBwcQUnroll
+      for (int q = 0; q < G::BPT; ++q) {
+        const int b = tid + q * NT;
+        if (!FC && b >= nbk) break;
+        const U* __restrict__ sv = reinterpret_cast<const U*>(s_val + hv) + b * E;
+        Word* __restrict__ dst = reinterpret_cast<Word*>(s_img + hw + (std::uint32_t)b * BB);
+        Word* ep = reinterpret_cast<Word*>(j.exps) + (b0 + (std::uint64_t)b);
+        if (FC) {
+          U u[E];
 #pragma unroll
-    for (int q = 0; q < G::BPT; ++q) {
-      const int b = tid + q * NT;
-      if (b >= nbk) break;
-      const U* __restrict__ sv = reinterpret_cast<const U*>(s_val + hv) + b * E;
-      Word* __restrict__ dst = reinterpret_cast<Word*>(s_img + hw + (std::uint32_t)b * BB);
-      U u[E];
-      std::int64_t be;
-      if ((b + 1) * E <= nv) {
-#pragma unroll
-        for (int k = 0; k < E; ++k) u[k] = sv[k];
-        bool plain;
-        be = bwc_block_exponent<T, BITS, E, true>(u, E, plain);
-        bwc_pack_block<T, BITS, E, true>(u, E, be, plain, dst);
-      } else { // the array's last block, partial
-        const int cnt = nv - b * E;
-#pragma unroll
-        for (int k = 0; k < E; ++k) u[k] = k < cnt ? sv[k] : U(0);
-        bool plain;
-        be = bwc_block_exponent<T, BITS, E, false>(u, cnt, plain);
-        bwc_pack_block<T, BITS, E, false>(u, cnt, be, plain, dst);
+          for (int k = 0; k < E; ++k) u[k] = sv[k];
+          bool plain;
+          const std::int64_t be = bwc_block_exponent<T, BITS, E, true>(u, E, plain);
+          if (__all_sync(0xffffffffu, plain)) {
+            bwc_pack_block<T, BITS, E, true, 1>(u, E, be, true, dst);
+            *ep = (Word)be;
+          } else {
+            bwc_compress_block_any<T, BITS, E>(sv, E, dst, ep);
+          }
+        } else {
+          bwc_compress_block_any<T, BITS, E>(sv, min(E, nv - b * E), dst, ep);
+        }
       }
-      reinterpret_cast<Word*>(j.exps)[b0 + (std::uint64_t)b] = (Word)be;
-    }
+    };
+    if (nv == NBC * E)
+      code_blocks(std::true_type{});
+    else
+      code_blocks(std::false_type{});
     __syncthreads();
-    const int last_cnt = nv - (nbk - 1) * E;
-    const std::uint32_t out_bytes = (std::uint32_t)(nbk - 1) * BB + written_block_bytes(last_cnt, BITS, W);
-    chunk_copy<true>(gout, s_img, out_bytes);
+    if (fast) {
+      bwc_store_full<NT, G::IMG_BYTES>(gout, s_img);
+    } else {
+      const int last_cnt = nv - (nbk - 1) * E;
+      const std::uint32_t out_bytes = (std::uint32_t)(nbk - 1) * BB + written_block_bytes(last_cnt, BITS, W);
+      chunk_copy<true>(gout, s_img, out_bytes);
+    }
     // no barrier here: the next chunk's commit writes the values region,
     // which every thread finished reading before the barrier above
   }
 }
 
 template<class T, int BITS, int E>
-__global__ void __launch_bounds__(bw_threads<T>()) k_decompress_bwc(Job j)
+__global__ void FRSZ2_BWC_BOUNDS_D(bw_threads<T>()) k_decompress_bwc(Job j)
 {
-  using G = bwc_cfg<T, BITS, E>;
+  using G = bwc_cfg<T, BITS, E, false>;
   using U = typename fp<T>::U;
   using Cfg = fast_cfg<T, BITS>;
   using C = typename Cfg::C;
@@ -218,6 +402,9 @@ __global__ void __launch_bounds__(bw_threads<T>()) k_decompress_bwc(Job j)
   };
   uint4 r[G::LOADS_I];
   std::int64_t be[G::BPT];
+  // chunk starts are 16-byte multiples apart on both sides, as in compress
+  static_assert((G::VAL_BYTES % 16) == 0 && (G::IMG_BYTES % 16) == 0, "chunk sizes");
+  const bool aligned = ((reinterpret_cast<std::uintptr_t>(y) | reinterpret_cast<std::uintptr_t>(j.words)) & 15u) == 0;
   auto issue = [&](std::uint64_t ch) {
     int nv, nbk;
     const std::uint64_t b0 = blocks_of(ch, nv, nbk);
@@ -227,7 +414,10 @@ __global__ void __launch_bounds__(bw_threads<T>()) k_decompress_bwc(Job j)
       if (b < nbk) be[q] = (std::int64_t)reinterpret_cast<const SWord*>(j.exps)[b0 + (std::uint64_t)b];
     }
     // whole blocks: the buffer holds every block in full
-    bw_issue<NT, G::LOADS_I>(j.words + b0 * (std::uint64_t)BB, (std::uint32_t)nbk * BB, r);
+    if (aligned && nv == NBC * E)
+      bwc_issue_full<NT, G::LOADS_I, G::IMG_BYTES>(j.words + b0 * (std::uint64_t)BB, r);
+    else
+      bw_issue<NT, G::LOADS_I>(j.words + b0 * (std::uint64_t)BB, (std::uint32_t)nbk * BB, r);
   };
   std::uint64_t ch = blockIdx.x;
   if (ch < nchunks) issue(ch);
@@ -238,52 +428,71 @@ __global__ void __launch_bounds__(bw_threads<T>()) k_decompress_bwc(Job j)
     std::uint8_t* gout = reinterpret_cast<std::uint8_t*>(y + b0 * (std::uint64_t)E);
     const std::uint32_t hw = (std::uint32_t)(reinterpret_cast<std::uintptr_t>(gin) & 15u);
     const std::uint32_t hv = (std::uint32_t)(reinterpret_cast<std::uintptr_t>(gout) & 15u);
-    bw_commit<NT, G::LOADS_I>(gin, s_img, (std::uint32_t)nbk * BB, r);
+    const bool fast = aligned && nv == NBC * E;
+    if (fast)
+      bwc_commit_full<NT, G::LOADS_I, G::IMG_BYTES>(s_img, r);
+    else
+      bw_commit<NT, G::LOADS_I>(gin, s_img, (std::uint32_t)nbk * BB, r);
     std::int64_t ecur[G::BPT];
 #pragma unroll
     for (int q = 0; q < G::BPT; ++q) ecur[q] = be[q];
     __syncthreads();
     if (ch + gridDim.x < nchunks) issue(ch + gridDim.x); // in flight while this chunk decodes
+    // A thread's blocks, each decoded by its own exponent's arithmetic (a
+    // warp vote and out-of-line rare paths, as compress uses, measured slower
+    // here, and so did a conversion-free plain-range decode, the fused
+    // multiply-add counterpart of compress's).  Full chunks skip the bounds
+    // and partial-block tests.
+    auto decode_blocks = [&](auto full_chunk) {
+      constexpr bool FC = decltype(full_chunk)::value;
 #pragma unroll
-    for (int q = 0; q < G::BPT; ++q) {
-      const int b = tid + q * NT;
-      if (b >= nbk) break;
-      const std::int64_t e = ecur[q];
-      const Word* src = reinterpret_cast<const Word*>(s_img + hw + (std::uint32_t)b * BB);
-      Word wd[NW];
+      for (int q = 0; q < G::BPT; ++q) {
+        const int b = tid + q * NT;
+        if (!FC && b >= nbk) break;
+        const std::int64_t e = ecur[q];
+        const Word* src = reinterpret_cast<const Word*>(s_img + hw + (std::uint32_t)b * BB);
+        Word wd[NW];
 #pragma unroll
-      for (int w = 0; w < NW; ++w) wd[w] = src[w];
-      U* sv = reinterpret_cast<U*>(s_val + hv) + b * E;
-      const int cnt = min(E, nv - b * E);
-      // full blocks store all E values; the array's last block, when partial,
-      // only its cnt
-      auto unpack = [&](auto decode, auto full) {
+        for (int w = 0; w < NW; ++w) wd[w] = src[w];
+        U* sv = reinterpret_cast<U*>(s_val + hv) + b * E;
+        const int cnt = FC ? E : min(E, nv - b * E);
+        // full blocks store all E values; the array's last block, when
+        // partial, only its cnt
+        auto unpack = [&](auto decode, auto full) {
 #pragma unroll
-        for (int k = 0; k < E; ++k) {
-          if (!decltype(full)::value && k >= cnt) break;
-          const int p = k * BITS, w = p / W, o = p % W; // constants after unrolling
-          C c = (C)((C)wd[w] >> o);
-          if (o + BITS > W) c |= (C)((C)wd[w + 1] << (W - o));
-          sv[k] = decode((C)(c & CMASK));
-        }
-      };
-      auto run = [&](auto full) {
-        if (plain_exponent<T>(e)) {
-          const T inv = pow2<T>((int)e - BITS + 2);
-          const U zero_bits =
-            sizeof(T) == 4 ? (U)((std::uint32_t)(e + 96) << 23) : (U)((std::uint64_t)(e + 992) << 52);
-          unpack([&](C c) { return decode_plain<T, BITS>(c, inv, zero_bits); }, full);
-        } else {
-          unpack([&](C c) { return to_bits<T>(from_code<T>((U)c, e, BITS)); }, full);
-        }
-      };
-      if (cnt == E)
-        run(std::true_type{});
-      else
-        run(std::false_type{});
-    }
+          for (int k = 0; k < E; ++k) {
+            if (!decltype(full)::value && k >= cnt) break;
+            const int p = k * BITS, w = p / W, o = p % W; // constants after unrolling
+            C c = (C)((C)wd[w] >> o);
+            if (o + BITS > W) c |= (C)((C)wd[w + 1] << (W - o));
+            sv[k] = decode((C)(c & CMASK));
+          }
+        };
+        auto run = [&](auto full) {
+          if (plain_exponent<T>(e)) {
+            const T inv = pow2<T>((int)e - BITS + 2);
+            const U zero_bits =
+              sizeof(T) == 4 ? (U)((std::uint32_t)(e + 96) << 23) : (U)((std::uint64_t)(e + 992) << 52);
+            unpack([&](C c) { return decode_plain<T, BITS>(c, inv, zero_bits); }, full);
+          } else {
+            unpack([&](C c) { return to_bits<T>(from_code<T>((U)c, e, BITS)); }, full);
+          }
+        };
+        if (FC || cnt == E)
+          run(std::true_type{});
+        else
+          run(std::false_type{});
+      }
+    };
+    if (nv == NBC * E)
+      decode_blocks(std::true_type{});
+    else
+      decode_blocks(std::false_type{});
     __syncthreads();
-    chunk_copy<true>(gout, s_val, (std::uint32_t)nv * (std::uint32_t)sizeof(T));
+    if (fast)
+      bwc_store_full<NT, G::VAL_BYTES>(gout, s_val);
+    else
+      chunk_copy<true>(gout, s_val, (std::uint32_t)nv * (std::uint32_t)sizeof(T));
     // no barrier here: the next chunk's commit writes the image region,
     // which every thread finished reading before the barrier above
   }
@@ -294,27 +503,28 @@ __global__ void __launch_bounds__(bw_threads<T>()) k_decompress_bwc(Job j)
 template<class T, int BITS, int E>
 cudaError_t launch_bwc_one(bool compress, const Job& j, cudaStream_t s)
 {
-  using G = bwc_cfg<T, BITS, E>;
+  using GC = bwc_cfg<T, BITS, E, true>;
+  using GD = bwc_cfg<T, BITS, E, false>;
   static std::atomic<int> resident[2];
   std::atomic<int>& slot = resident[compress ? 0 : 1];
   int per_sm = slot.load(std::memory_order_relaxed);
   if (per_sm == 0) {
     int n = 0;
     const cudaError_t e = compress
-                            ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_compress_bwc<T, BITS, E>, G::NT, 0)
-                            : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_decompress_bwc<T, BITS, E>, G::NT, 0);
+                            ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_compress_bwc<T, BITS, E>, GC::NT, 0)
+                            : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_decompress_bwc<T, BITS, E>, GD::NT, 0);
     if (e != cudaSuccess) return e;
     per_sm = n < 1 ? 1 : n;
     slot.store(per_sm, std::memory_order_relaxed);
   }
   const std::uint64_t nb = (j.n + (std::uint64_t)E - 1) / (std::uint64_t)E;
   const std::uint64_t ctas = (std::uint64_t)sm_count() * (std::uint64_t)per_sm;
-  const unsigned grid =
-    (unsigned)std::max<std::uint64_t>(1, std::min<std::uint64_t>((nb + G::NBC - 1) / G::NBC, ctas));
+  const std::uint64_t nbc = compress ? (std::uint64_t)GC::NBC : (std::uint64_t)GD::NBC;
+  const unsigned grid = (unsigned)std::max<std::uint64_t>(1, std::min<std::uint64_t>((nb + nbc - 1) / nbc, ctas));
   if (compress)
-    k_compress_bwc<T, BITS, E><<<grid, G::NT, 0, s>>>(j);
+    k_compress_bwc<T, BITS, E><<<grid, GC::NT, 0, s>>>(j);
   else
-    k_decompress_bwc<T, BITS, E><<<grid, G::NT, 0, s>>>(j);
+    k_decompress_bwc<T, BITS, E><<<grid, GD::NT, 0, s>>>(j);
   return cudaGetLastError();
 }
 
