@@ -255,3 +255,38 @@ def test_compile_time_block_sizes_off_alignment(cuda, E):
             want = oracle.decompress(ref, n, dtype, bits, E)
             assert np.array_equal(got[voff:voff + n].view(uint), want.view(uint)), (dtype, bits, voff, boff)
             assert np.all(got[:voff] == -7.0) and np.all(got[voff + n:] == -7.0)
+
+
+def top_of_range_values(dtype, n, seed):
+    """Blocks of 32 whose values have every mantissa bit set (and their
+    neighbours one ulp down), at random exponents across the plain range and
+    random signs, mixed with zeros, subnormals and values far below the block
+    maximum: the codes reach 2^(bits-1) - 1, the largest magnitude the plain
+    range encodes."""
+    rng = np.random.default_rng(seed)
+    fi = np.finfo(dtype)
+    ones = dtype(2.0) - fi.eps  # 1.111...1 in binary
+    lo, hi = (-90, 120) if dtype == np.float32 else (-950, 1000)
+    x = np.empty(n, dtype=dtype)
+    for b in range(0, n, 32):
+        e = int(rng.integers(lo, hi))
+        blk = (ones * np.power(dtype(2.0), dtype(e))).astype(dtype) * np.ones(32, dtype=dtype)
+        blk[1::3] = np.nextafter(blk[1::3], dtype(0))
+        blk[2::5] = blk[2::5] * dtype(2.0) ** -int(rng.integers(1, 40))
+        blk[3] = 0.0
+        blk[4] = float(fi.tiny) * 0.5 if e > lo + 40 else blk[4]
+        blk *= np.where(rng.random(32) < 0.5, -1, 1).astype(dtype)
+        x[b:b + 32] = blk[: min(32, n - b)]
+    return x
+
+
+@pytest.mark.parametrize("dtype,bits", [(np.float32, b) for b in (4, 8, 13, 16, 23, 24, 25, 32)] +
+                         [(np.float64, b) for b in (4, 16, 31, 32, 33, 52, 53, 54, 64)])
+def test_plain_range_top_codes(cuda, dtype, bits):
+    """The largest magnitudes of the plain range (codes up to 2^(bits-1) - 1)
+    on the fast and the blockwise kernels, around the widths where the
+    fused multiply-add truncation stops (24 for fp32, 53 for fp64)."""
+    n = 4 * 4096 + 77
+    x = top_of_range_values(dtype, n, bits)
+    for E in (32, 5, 8):
+        check(x, bits, E)
