@@ -3,6 +3,7 @@
 #include "frsz2_blockvec.cuh"
 #include "frsz2_blockwise.cuh"
 #include "frsz2_chunked.cuh"
+#include "frsz2_chunked_ct.cuh"
 #include "frsz2_fast_dispatch.hpp"
 #include "frsz2_kernels.cuh"
 #include "frsz2_launch.hpp"
@@ -155,14 +156,6 @@ static Job job_from_block(const Job& j, std::uint64_t b0, std::size_t es)
   return t;
 }
 
-// One CTA per chunk of whole blocks (frsz2_chunked.cuh).
-static unsigned chunk_grid(const Job& j)
-{
-  const std::uint64_t nb = (j.n + (std::uint64_t)j.E - 1) / (std::uint64_t)j.E;
-  const std::uint64_t nbc = (std::uint64_t)chunk_blocks(j.E);
-  return (unsigned)std::max<std::uint64_t>(1, std::min<std::uint64_t>((nb + nbc - 1) / nbc, 1u << 30));
-}
-
 template<class T>
 static int launch_compress_t(const Job& j, int dtype, cudaStream_t s, bool* used_tile)
 {
@@ -190,6 +183,10 @@ static int launch_compress_t(const Job& j, int dtype, cudaStream_t s, bool* used
                                          : launch_blockvec_f32(j.bits, j, full, s);
     if (e != cudaSuccess) return cuda_status(e, "compress launch");
     if (full * (std::uint64_t)j.E < j.n) k_compress_generic<T><<<1, kNT, 0, s>>>(job_from_block(j, full, sizeof(T)));
+  } else if (chunked_ct_eligible(j)) {
+    return cuda_status(sizeof(T) == 8 ? launch_chunked_ct_f64(j.bits, true, j, s)
+                                      : launch_chunked_ct_f32(j.bits, true, j, s),
+                       "compress launch");
   } else {
     const std::uint64_t nb = (j.n + (std::uint64_t)j.E - 1) / (std::uint64_t)j.E;
     k_compress_generic<T><<<grid_for(nb, kNT / 32), kNT, 0, s>>>(j);
@@ -218,11 +215,10 @@ static int launch_decompress_t(const Job& j, int dtype, cudaStream_t s, bool* us
     return cuda_status(sizeof(T) == 8 ? launch_blockwise_f64(j.bits, false, j, s)
                                       : launch_blockwise_f32(j.bits, false, j, s),
                        "decompress launch");
-  } else if (j.E <= kChunkMaxEDecompress) {
-    if (j.bits <= 32)
-      k_decompress_chunked<T, std::uint32_t><<<chunk_grid(j), kNT, 0, s>>>(j);
-    else
-      k_decompress_chunked<T, std::uint64_t><<<chunk_grid(j), kNT, 0, s>>>(j);
+  } else if (chunked_ct_eligible(j)) {
+    return cuda_status(sizeof(T) == 8 ? launch_chunked_ct_f64(j.bits, false, j, s)
+                                      : launch_chunked_ct_f32(j.bits, false, j, s),
+                       "decompress launch");
   } else {
     const std::uint64_t nb = (j.n + (std::uint64_t)j.E - 1) / (std::uint64_t)j.E;
     k_decompress_generic<T><<<grid_for(nb, kNT / 32), kNT, 0, s>>>(j);

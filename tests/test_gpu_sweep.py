@@ -290,3 +290,55 @@ def test_plain_range_top_codes(cuda, dtype, bits):
     x = top_of_range_values(dtype, n, bits)
     for E in (32, 5, 8):
         check(x, bits, E)
+
+
+@pytest.mark.parametrize("dtype,bits", [(np.float32, b) for b in range(4, 33)] + [(np.float64, b) for b in range(4, 65)])
+def test_blocks_17_to_128_every_width(cuda, dtype, bits):
+    """Block sizes 17..128 that are not powers of two (the compile-time-width
+    chunked kernels): several chunks, a partial last block, special values,
+    values pointers off 16-byte alignment; compressed bytes equal the
+    oracle's, nothing written outside the buffer or the output."""
+    es = np.dtype(dtype).itemsize
+    tdt = torch.float32 if es == 4 else torch.float64
+    uint = np.uint32 if es == 4 else np.uint64
+    for E in (17, 33, 100, 128 - (bits % 3)):
+        n = 5 * 2048 + 2 * E + E // 3 + 1
+        x = special_values(dtype, n, bits * 29 + E)
+        ref = oracle.compress(x, bits, E, canary=0x44)
+        want = oracle.decompress(ref, n, dtype, bits, E)
+        size = ref.size
+        for voff in (0, 1):
+            tv = torch.zeros(n + 4, dtype=tdt, device="cuda")
+            tv[voff:voff + n] = torch.from_numpy(x).cuda()
+            buf = torch.full((size,), 0x44, dtype=torch.uint8, device="cuda")
+            frsz_b200.compress(tv[voff:voff + n], bits, E, out=buf)
+            got = buf.cpu().numpy()
+            if not np.array_equal(got, ref):
+                bad = np.flatnonzero(got != ref)
+                raise AssertionError(f"bits={bits} E={E} voff={voff}: {bad.size} bytes differ, first {bad[:6]}")
+        for voff in (0, 1):
+            out = torch.full((n + 4,), -7.0, dtype=tdt, device="cuda")
+            frsz_b200.decompress(torch.from_numpy(ref).cuda(), n, dtype, bits, E, out=out[voff:voff + n])
+            got = out.cpu().numpy()
+            assert np.array_equal(got[voff:voff + n].view(uint), want.view(uint)), (bits, E, voff)
+            assert np.all(got[:voff] == -7.0) and np.all(got[voff + n:] == -7.0), (bits, E, voff)
+
+
+@pytest.mark.parametrize("E", [17, 19, 24, 48, 100, 127, 128 - 1])
+def test_blocks_17_to_128_whole_chunks(cuda, E):
+    """Arrays of exactly whole chunks (the chunked kernels take 2048 // E
+    blocks at a time, so a chunk holds up to E - 1 values fewer than 2048):
+    the last chunk is full and nothing is written past the array."""
+    for dtype, bits in ((np.float32, 16), (np.float32, 5), (np.float64, 21), (np.float64, 40)):
+        es = np.dtype(dtype).itemsize
+        tdt = torch.float32 if es == 4 else torch.float64
+        uint = np.uint32 if es == 4 else np.uint64
+        n = (2048 // E) * E * 3
+        x = special_values(dtype, n, bits + E)
+        check(x, bits, E)
+        ref = oracle.compress(x, bits, E, canary=0x44)
+        out = torch.full((n + 256,), -7.0, dtype=tdt, device="cuda")
+        frsz_b200.decompress(torch.from_numpy(ref).cuda(), n, dtype, bits, E, out=out[:n])
+        got = out.cpu().numpy()
+        assert np.array_equal(got[:n].view(uint), oracle.decompress(ref, n, dtype, bits, E).view(uint)), (bits, E)
+        assert np.all(got[n:] == -7.0), (bits, E)
