@@ -35,7 +35,8 @@ class BatchStatsC(ctypes.Structure):
                 ("separate_launches", ctypes.c_uint64), ("classes", ctypes.c_uint64),
                 ("tiles", ctypes.c_uint64 * 2), ("threads_per_cta", ctypes.c_int * 2),
                 ("rows_per_warp", ctypes.c_int * 2), ("ctas_per_sm", ctypes.c_int * 2),
-                ("side_by_side", ctypes.c_int * 2), ("tuned", ctypes.c_int * 2)]
+                ("side_by_side", ctypes.c_int * 2), ("tuned", ctypes.c_int * 2),
+                ("one_cta_per_tile", ctypes.c_int * 2)]
 
 
 class RequestC(ctypes.Structure):
@@ -81,6 +82,7 @@ SIGNATURES = {
     "frsz2_batch_compress": (_int, [_vp, _vp]),
     "frsz2_batch_decompress": (_int, [_vp, _vp]),
     "frsz2_batch_autotune": (_int, [_vp, _int, _vp, ctypes.POINTER(ctypes.c_float)]),
+    "frsz2_batch_configure": (_int, [_vp, _int, _int, _int, _int, _int]),
     "frsz2_batch_info": (_int, [_vp, ctypes.POINTER(BatchStatsC)]),
     "frsz2_batch_destroy": (None, [_vp]),
     "frsz2_batch_compress_static": (_int, [ctypes.POINTER(BatchItemC), _u64, _vp]),

@@ -66,11 +66,19 @@ class BatchPlan:
         check(lib().frsz2_batch_autotune(self._h, int(compress), self._stream(stream), ctypes.byref(ms)))
         return ms.value
 
+    def configure(self, compress: bool, shape: int = 0, ctas_per_sm: int = 4, side_by_side: bool = False,
+                  one_cta_per_tile: bool = False) -> None:
+        """Set one direction's launch configuration by hand
+        (frsz2_batch_configure)."""
+        check(lib().frsz2_batch_configure(self._h, int(compress), shape, ctas_per_sm, int(side_by_side),
+                                          int(one_cta_per_tile)))
+
     def info(self) -> dict:
         st = BatchStatsC()
         check(lib().frsz2_batch_info(self._h, ctypes.byref(st)))
         out = {k: getattr(st, k) for k in ("arrays", "persistent_arrays", "separate_launches", "classes")}
-        for k in ("tiles", "threads_per_cta", "rows_per_warp", "ctas_per_sm", "side_by_side", "tuned"):
+        for k in ("tiles", "threads_per_cta", "rows_per_warp", "ctas_per_sm", "side_by_side", "tuned",
+                  "one_cta_per_tile"):
             v = getattr(st, k)
             out[k] = {"decompress": v[0], "compress": v[1]}
         return out

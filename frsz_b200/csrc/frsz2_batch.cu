@@ -1,9 +1,12 @@
 // frsz2_batch.cu -- many arrays of mixed float types, widths and sizes per
-// call: one CUDA graph launch whose parallel branches are persistent kernels,
-// one per (float type, width) class present in the batch, each walking its
-// class's device-resident work list.  An autotuner picks the CTA shape, the
-// number of resident CTAs per SM and whether classes run side by side or one
-// after another, by timing the candidates on the plan's own arrays.
+// call: one CUDA graph launch whose parallel branches are one kernel per
+// (float type, width) class present in the batch, over the class's
+// device-resident work list: one CTA per tile (the tile's array from a
+// per-tile index; the default) or a persistent grid walking the class's
+// tiles.  An autotuner picks between them, and the CTA shape, the number of
+// resident CTAs per SM of the persistent grid and whether classes run side by
+// side or one after another, by timing the candidates on the plan's own
+// arrays.
 //
 // One kernel per class rather than one kernel switching over widths: a
 // multi-width kernel gets a register allocation sized for the union of its
@@ -30,6 +33,7 @@ struct Class
   std::vector<int> items;                         // plan item indices
   std::uint64_t tiles[kNumShapes] = { 0, 0, 0 };
   std::size_t desc_off[kNumShapes] = { 0, 0, 0 }; // first descriptor in the shape's array
+  std::uint64_t tmap_off = 0;                     // first entry of the shape-0 tile index
   batch_entry entry[kNumShapes] = {};
 };
 
@@ -44,11 +48,14 @@ struct frsz2_batch
   std::vector<Class> classes;
   std::vector<int> other_items; // items with their own launch
   BatchItem* d_desc[kNumShapes] = { nullptr, nullptr, nullptr };
+  // shape 0, per tile of every class: the tile's descriptor within its class
+  std::uint32_t* d_tmap = nullptr;
   bool shape_ok[kNumShapes] = { false, false, false };
   // launch configuration per direction (0 = decompress, 1 = compress)
   int shape[2] = { 0, 0 };
   int ctas_per_sm[2] = { 0, 0 };
   int parallel[2] = { 1, 1 };
+  int per_tile[2] = { 0, 0 }; // 1: one CTA per tile (shape 0), not the persistent class kernels
   bool tuned[2] = { false, false };
   cudaGraphExec_t graph[2] = { nullptr, nullptr };
   cudaStream_t branch[kMaxBranches] = {};
@@ -85,8 +92,11 @@ int ensure_branches(frsz2_batch* p)
   return FRSZ2_OK;
 }
 
-// Enqueue one direction on stream s with the given configuration.
-int enqueue(frsz2_batch* p, bool compress, cudaStream_t s, int shape, int ctas_per_sm, bool parallel)
+// Enqueue one direction on stream s with the given configuration; per_tile
+// launches one CTA per tile of each class (shape 0) instead of the
+// persistent class kernels.
+int enqueue(frsz2_batch* p, bool compress, cudaStream_t s, int shape, int ctas_per_sm, bool parallel,
+            bool per_tile = false)
 {
   const std::uint64_t total = class_tiles_total(p, shape);
   const std::uint64_t ctas = (std::uint64_t)sm_count() * (std::uint64_t)ctas_per_sm;
@@ -105,8 +115,11 @@ int enqueue(frsz2_batch* p, bool compress, cudaStream_t s, int shape, int ctas_p
     std::uint64_t grid = fork ? (ctas * tiles + total - 1) / total : ctas;
     grid = std::max<std::uint64_t>(1, std::min(grid, tiles));
     cudaStream_t st = fork ? p->branch[ci % nb] : s;
-    const cudaError_t e = c.entry[shape].launch(compress, p->d_desc[shape] + c.desc_off[shape], (int)c.items.size(),
-                                                tiles, (unsigned)grid, st);
+    const cudaError_t e =
+      per_tile && shape == 0 && c.entry[0].launch_tiles && p->d_tmap
+        ? c.entry[0].launch_tiles(compress, p->d_desc[0] + c.desc_off[0], p->d_tmap + c.tmap_off, tiles, st)
+        : c.entry[shape].launch(compress, p->d_desc[shape] + c.desc_off[shape], (int)c.items.size(), tiles,
+                                (unsigned)grid, st);
     if (int rc = cuda_status(e, "batch launch")) return rc;
   }
   if (fork) {
@@ -138,7 +151,7 @@ int build_graph(frsz2_batch* p, bool compress)
   cudaGraph_t g = nullptr;
   rc = cuda_status(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal), "begin capture");
   if (!rc) {
-    rc = enqueue(p, compress, cs, p->shape[d], p->ctas_per_sm[d], p->parallel[d] != 0);
+    rc = enqueue(p, compress, cs, p->shape[d], p->ctas_per_sm[d], p->parallel[d] != 0, p->per_tile[d] != 0);
     const int rc2 = cuda_status(cudaStreamEndCapture(cs, &g), "end capture");
     if (!rc) rc = rc2;
   }
@@ -149,14 +162,17 @@ int build_graph(frsz2_batch* p, bool compress)
 }
 
 // Untuned configuration: what the autotuner picked for the 4096-array mixed
-// batch (256 x 2 CTAs, classes one after another, 4 resident CTAs per SM);
-// side by side with every resident CTA measured 30 % slower on compress.
+// batch: one CTA per tile (256 x 2), classes side by side (0.95 of HBM, against
+// 0.90 for the persistent class kernels, 4 resident CTAs per SM, classes one
+// after another, which the autotuner picked before the per-tile launch
+// existed).  Plans without the tile index keep the persistent kernels.
 void default_config(frsz2_batch* p, bool compress)
 {
   const int d = compress ? 1 : 0;
   p->shape[d] = 0;
   p->ctas_per_sm[d] = p->classes.empty() ? 1 : std::min(4, min_occupancy(p, 0, compress));
-  p->parallel[d] = 0;
+  p->per_tile[d] = p->d_tmap && p->shape_ok[0] ? 1 : 0;
+  p->parallel[d] = p->per_tile[d];
 }
 
 int check_direction(const frsz2_batch* p, bool compress)
@@ -192,7 +208,7 @@ int autotune(frsz2_batch* p, bool compress, cudaStream_t s, float* best_ms_out)
     return rc;
   }
   float best = 1e30f;
-  int best_shape = p->shape[d], best_ctas = p->ctas_per_sm[d], best_par = p->parallel[d];
+  int best_shape = p->shape[d], best_ctas = p->ctas_per_sm[d], best_par = p->parallel[d], best_tile = p->per_tile[d];
   const int modes = p->classes.size() > 1 ? 2 : 1;
   for (int shape = 0; shape < kNumShapes && !rc; ++shape) {
     if (!p->shape_ok[shape] || p->classes.empty()) continue;
@@ -218,8 +234,31 @@ int autotune(frsz2_batch* p, bool compress, cudaStream_t s, float* best_ms_out)
           best_shape = shape;
           best_ctas = c;
           best_par = par ? 1 : 0;
+          best_tile = 0;
         }
       }
+    }
+  }
+  // one CTA per tile (shape 0), classes side by side or one after another
+  for (int m = 0; m < modes && !rc && p->d_tmap && p->shape_ok[0] && !p->classes.empty(); ++m) {
+    const bool par = m == 0;
+    if ((rc = enqueue(p, compress, s, 0, 1, par, true))) break; // warm
+    float ms_min = 1e30f;
+    for (int rep = 0; rep < 3 && !rc; ++rep) {
+      cudaEventRecord(a, s);
+      rc = enqueue(p, compress, s, 0, 1, par, true);
+      cudaEventRecord(b, s);
+      if (!rc) rc = cuda_status(cudaEventSynchronize(b), "autotune sync");
+      float ms = 0;
+      if (!rc) cudaEventElapsedTime(&ms, a, b);
+      ms_min = std::min(ms_min, ms);
+    }
+    if (!rc && ms_min < best) {
+      best = ms_min;
+      best_shape = 0;
+      best_ctas = p->ctas_per_sm[d];
+      best_par = par ? 1 : 0;
+      best_tile = 1;
     }
   }
   cudaEventDestroy(a);
@@ -228,6 +267,7 @@ int autotune(frsz2_batch* p, bool compress, cudaStream_t s, float* best_ms_out)
   p->shape[d] = best_shape;
   p->ctas_per_sm[d] = best_ctas;
   p->parallel[d] = best_par;
+  p->per_tile[d] = best_tile;
   p->tuned[d] = true;
   if (best_ms_out) *best_ms_out = best;
   return build_graph(p, compress);
@@ -318,6 +358,26 @@ int frsz2_batch_create(const frsz2_batch_item* items, uint64_t count, frsz2_batc
       return rc;
     }
   }
+  if (p->shape_ok[0]) {
+    std::vector<std::uint32_t> tmap;
+    for (auto& c : p->classes) {
+      c.tmap_off = tmap.size();
+      for (std::size_t k = 0; k < c.items.size(); ++k) {
+        const frsz2_batch_item& it = p->items[c.items[k]];
+        const int tv = fast_tile_values(c.is64 ? 8 : 4, kShapes[0].nt, kShapes[0].rpw);
+        tmap.insert(tmap.end(), (it.n + (std::uint64_t)tv - 1) / (std::uint64_t)tv, (std::uint32_t)k);
+      }
+    }
+    int rc = cuda_status(cudaMalloc(&p->d_tmap, std::max<std::size_t>(1, tmap.size()) * sizeof(std::uint32_t)),
+                         "tile index allocation");
+    if (!rc && !tmap.empty())
+      rc = cuda_status(cudaMemcpy(p->d_tmap, tmap.data(), tmap.size() * sizeof(std::uint32_t), cudaMemcpyHostToDevice),
+                       "tile index upload");
+    if (rc) {
+      frsz2_batch_destroy(p);
+      return rc;
+    }
+  }
   if (!p->classes.empty() && !p->shape_ok[0]) {
     // block sizes too large for the default tile: every array gets its own launch
     for (auto& c : p->classes) p->other_items.insert(p->other_items.end(), c.items.begin(), c.items.end());
@@ -355,6 +415,27 @@ int frsz2_batch_autotune(frsz2_batch* plan, int compress, void* stream, float* b
   return autotune(plan, compress != 0, static_cast<cudaStream_t>(stream), best_ms);
 }
 
+int frsz2_batch_configure(frsz2_batch* plan, int compress, int shape, int ctas_per_sm, int side_by_side,
+                          int one_cta_per_tile)
+{
+  if (!plan) return set_error(FRSZ2_EFAIL, "null plan");
+  std::lock_guard<std::mutex> lock(plan->mu);
+  if (shape < 0 || shape >= kNumShapes || !plan->shape_ok[shape])
+    return set_error(FRSZ2_EFAIL, "launch shape " + std::to_string(shape) + " is not available for this plan");
+  if (one_cta_per_tile && (shape != 0 || !plan->d_tmap))
+    return set_error(FRSZ2_EFAIL, "one CTA per tile needs launch shape 0");
+  const int occ = plan->classes.empty() ? 1 : min_occupancy(plan, shape, compress != 0);
+  if (ctas_per_sm < 1 || ctas_per_sm > occ)
+    return set_error(FRSZ2_EFAIL, "ctas_per_sm must be 1.." + std::to_string(occ) + " for this plan and shape");
+  const int d = compress ? 1 : 0;
+  plan->shape[d] = shape;
+  plan->ctas_per_sm[d] = ctas_per_sm;
+  plan->parallel[d] = side_by_side ? 1 : 0;
+  plan->per_tile[d] = one_cta_per_tile ? 1 : 0;
+  plan->tuned[d] = false;
+  return build_graph(plan, compress != 0);
+}
+
 int frsz2_batch_info(const frsz2_batch* plan, frsz2_batch_stats* out)
 {
   if (!plan || !out) return set_error(FRSZ2_EFAIL, "null pointer");
@@ -371,6 +452,7 @@ int frsz2_batch_info(const frsz2_batch* plan, frsz2_batch_stats* out)
     out->side_by_side[d] = plan->parallel[d];
     out->tiles[d] = class_tiles_total(plan, sh);
     out->tuned[d] = plan->tuned[d] ? 1 : 0;
+    out->one_cta_per_tile[d] = plan->per_tile[d];
   }
   return FRSZ2_OK;
 }
@@ -382,6 +464,7 @@ void frsz2_batch_destroy(frsz2_batch* plan)
     if (g) cudaGraphExecDestroy(g);
   for (auto& d : plan->d_desc)
     if (d) cudaFree(d);
+  if (plan->d_tmap) cudaFree(plan->d_tmap);
   for (int i = 0; i < kMaxBranches; ++i) {
     if (plan->branch[i]) cudaStreamDestroy(plan->branch[i]);
     if (plan->join[i]) cudaEventDestroy(plan->join[i]);

@@ -10,7 +10,8 @@ template<int LO, int... I>
 constexpr auto f32_shape0(std::integer_sequence<int, I...>)
 {
   return std::array<batch_entry, sizeof...(I)>{ batch_entry{ &launch_batch_class<float, LO + I, 256, 2>,
-                                                             &batch_class_occupancy<float, LO + I, 256, 2> }... };
+                                                             &batch_class_occupancy<float, LO + I, 256, 2>,
+                                                             &launch_batch_tiles<float, LO + I, 256, 2> }... };
 }
 
 batch_entry batch_class_f32(int bits, int shape)

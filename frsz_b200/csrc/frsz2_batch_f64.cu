@@ -10,7 +10,8 @@ template<int LO, int... I>
 constexpr auto f64_shape0(std::integer_sequence<int, I...>)
 {
   return std::array<batch_entry, sizeof...(I)>{ batch_entry{ &launch_batch_class<double, LO + I, 256, 2>,
-                                                             &batch_class_occupancy<double, LO + I, 256, 2> }... };
+                                                             &batch_class_occupancy<double, LO + I, 256, 2>,
+                                                             &launch_batch_tiles<double, LO + I, 256, 2> }... };
 }
 
 batch_entry batch_class_f64(int bits, int shape)

@@ -45,6 +45,48 @@ __global__ void __launch_bounds__(NT)
   }
 }
 
+// One CTA per tile of a class's concatenated tile list, the tile's array
+// read from a per-tile index (one 4-byte load): the launch shape of the
+// single-array kernels, which hardware CTA scheduling balances across SMs.
+template<class T, int BITS, int NT, int RPW, bool COMPRESS>
+__global__ void __launch_bounds__(NT)
+  k_batch_tiles(const BatchItem* __restrict__ items, const std::uint32_t* __restrict__ tile_item)
+{
+  __shared__ std::uint32_t s_rmax[2 * (NT / 32) * RPW];
+  __shared__ __align__(16) std::uint32_t s_stage[stage_words<T, BITS, NT, RPW>::value];
+  const std::uint64_t t = blockIdx.x;
+  const std::uint32_t it = __ldg(tile_item + t);
+  const Job j = items[it].job;
+  const std::uint64_t lt = t - items[it].tile_begin;
+  if constexpr (!fast_cfg<T, BITS, NT, RPW>::ALIGNED) {
+    if (job_padded(j)) {
+      if (COMPRESS)
+        fast_compress_tile<T, BITS, NT, RPW, true>(j, lt, s_rmax, s_stage, false);
+      else
+        fast_decompress_tile<T, BITS, NT, RPW, true>(j, lt);
+      return;
+    }
+  }
+  if (COMPRESS)
+    fast_compress_tile<T, BITS, NT, RPW>(j, lt, s_rmax, s_stage, false);
+  else
+    fast_decompress_tile<T, BITS, NT, RPW>(j, lt);
+}
+
+using batch_tiles_fn = cudaError_t (*)(bool compress, const BatchItem* items, const std::uint32_t* tile_item,
+                                       std::uint64_t tiles, cudaStream_t s);
+
+template<class T, int BITS, int NT, int RPW>
+cudaError_t launch_batch_tiles(bool compress, const BatchItem* items, const std::uint32_t* tile_item,
+                               std::uint64_t tiles, cudaStream_t s)
+{
+  if (compress)
+    k_batch_tiles<T, BITS, NT, RPW, true><<<(unsigned)tiles, NT, 0, s>>>(items, tile_item);
+  else
+    k_batch_tiles<T, BITS, NT, RPW, false><<<(unsigned)tiles, NT, 0, s>>>(items, tile_item);
+  return cudaGetLastError();
+}
+
 // CTA shapes the autotuner chooses from: (threads, rows per warp).  Shape 0
 // exists for every width; shapes 1 and 2 for the widths of FRSZ2_TUNED_WIDTHS.
 struct Shape
@@ -85,6 +127,7 @@ struct batch_entry
 {
   batch_fn launch;
   int (*occupancy)(bool);
+  batch_tiles_fn launch_tiles; // one CTA per tile (shape 0 only)
 };
 batch_entry batch_class_f32(int bits, int shape);
 batch_entry batch_class_f64(int bits, int shape);

@@ -26,11 +26,11 @@
  * <= 65536.  Device pointers must be aligned to their element / word type.
  * Speed: power-of-two block sizes from 8 (fp32) / 4 (fp64) values up with a
  * 32-byte aligned buffer run at about the HBM bandwidth; values off the
- * 32-byte layout (a view such as x + 1) at 0.7-0.9 of it; other block sizes
- * up to 16 values at 0.4-0.8; compress of block sizes 17-64 whose blocks
- * start on 16-byte boundaries at 0.2-0.7; other block sizes that are not
- * powers of two, or a buffer off the 32-byte layout, on slower general
- * kernels.
+ * 32-byte layout (a view such as x + 1) at 0.7-0.9 of it; block sizes 3, 5, 6,
+ * 7 and 12 at 0.74-1.0, other block sizes up to 16 values at 0.4-0.8; block
+ * sizes 17-128 decompress at 0.33-0.89 and compress at 0.2-0.7; larger block
+ * sizes that are not powers of two, or a buffer off the 32-byte layout, on
+ * slower general kernels.
  */
 #ifndef FRSZ2_B200_H
 #define FRSZ2_B200_H
@@ -125,11 +125,13 @@ int frsz2_decompress_elements_host(int dtype, int bits, int block_size, const vo
 /* ---------------------------------------------------------------------------
  * Batched path: no counterpart in the reference (which compresses one array
  * per call).  Many arrays of mixed float types, widths, block sizes and sizes
- * run as one CUDA graph launch: a persistent kernel per (float type, width)
- * class present, side by side, each walking its class's work list in device
- * memory.  The launch shape (threads per CTA, rows per warp, resident CTAs
- * per SM, classes side by side or one after another) comes from an autotuner
- * that times the candidates on the plan's own arrays.  Arrays the persistent
+ * run as one CUDA graph launch: a kernel per (float type, width) class present,
+ * side by side, over its class's work list in device memory -- one CTA per
+ * tile (the default) or a persistent grid.  The launch configuration (one CTA
+ * per tile or persistent; threads per CTA, rows per warp, resident CTAs per SM;
+ * classes side by side or one after another) comes from an autotuner that
+ * times the candidates on the plan's own arrays, or from
+ * frsz2_batch_configure.  Arrays the persistent
  * kernels cannot take (block sizes that are not powers of two, block padding,
  * misaligned pointers) get their own launch inside the same graph.  All
  * pointers are device pointers; a plan keeps its descriptors in device memory
@@ -158,6 +160,7 @@ typedef struct frsz2_batch_stats {
   int ctas_per_sm[2];
   int side_by_side[2];        /* 1: classes run concurrently, 0: one after another */
   int tuned[2];
+  int one_cta_per_tile[2];    /* 1: one CTA per tile, 0: persistent kernels per class */
 } frsz2_batch_stats;
 
 int frsz2_batch_create(const frsz2_batch_item* items, uint64_t count, frsz2_batch** plan);
@@ -167,6 +170,14 @@ int frsz2_batch_decompress(frsz2_batch* plan, void* stream);
  * or decompress), keeps the fastest and rebuilds that direction's graph.  The
  * run writes the plan's outputs like a normal call.  *best_ms may be NULL. */
 int frsz2_batch_autotune(frsz2_batch* plan, int compress, void* stream, float* best_ms);
+/* Sets one direction's launch configuration by hand, as frsz2_batch_autotune
+ * would (for instance a configuration tuned once offline): shape 0..2 (256 x 2,
+ * 128 x 2, 512 x 1 threads x rows per warp), resident CTAs per SM, classes side
+ * by side (1) or one after another (0), and one CTA per tile (1, shape 0 only)
+ * instead of the persistent kernel per class (0).  Rebuilds that direction's
+ * graph; returns 2 for a configuration the plan cannot run. */
+int frsz2_batch_configure(frsz2_batch* plan, int compress, int shape, int ctas_per_sm, int side_by_side,
+                          int one_cta_per_tile);
 int frsz2_batch_info(const frsz2_batch* plan, frsz2_batch_stats* stats);
 void frsz2_batch_destroy(frsz2_batch* plan);
 

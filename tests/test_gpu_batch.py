@@ -158,3 +158,23 @@ def test_batch_views_off_32_bytes(cuda):
     torch.cuda.synchronize()
     check_batch(arrays, host)
     plan.close()
+
+
+@pytest.mark.parametrize("one_cta_per_tile,side_by_side", [(True, False), (True, True), (False, True)])
+def test_batch_launch_configurations(cuda, one_cta_per_tile, side_by_side):
+    """Every launch configuration gives the oracle's bytes and values: one CTA
+    per tile (the tile's array from a per-tile index) and the persistent
+    class kernels, classes one after another or side by side."""
+    arrays, host = make_batch(SPECS[:12], seed=11)
+    plan = BatchPlan(arrays)
+    for compress in (True, False):
+        plan.configure(compress, shape=0, ctas_per_sm=2, side_by_side=side_by_side,
+                       one_cta_per_tile=one_cta_per_tile)
+    info = plan.info()
+    assert info["one_cta_per_tile"] == {"decompress": int(one_cta_per_tile), "compress": int(one_cta_per_tile)}
+    plan.compress()
+    plan.decompress()
+    torch.cuda.synchronize()
+    check_batch(arrays, host)
+    with pytest.raises(frsz_b200.Frsz2Error, match="shape 0"):
+        plan.configure(True, shape=1, one_cta_per_tile=True)
