@@ -499,7 +499,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
     if rank != 0:
         return
 
-    # ---- the other north-star measurements, summarised in the same line (N = 1,
+    # ---- the batched, fused-basis and serving measurements, summarised in the same line (N = 1,
     # default workload): batched, fused basis dot / axpy, serving
     extras = None
     if world == 1 and args.extras and args.workload == DEFAULT_WORKLOAD:
@@ -689,7 +689,7 @@ def run_shard(args, rank: int, world: int, local_rank: int) -> None:
 # ---------------------------------------------------------------- batched
 
 def batched_specs(count: int = 4096, seed: int = 7):
-    """Config 4: byte sizes log-uniform in [1 KiB, 64 MiB], 50/50 fp32/fp64,
+    """The 4,096-array batch: byte sizes log-uniform in [1 KiB, 64 MiB], 50/50 fp32/fp64,
     bits uniform over {8, 12, 16, 24, 32}, block 32."""
     rng = np.random.default_rng(seed)
     specs = []
@@ -835,7 +835,7 @@ def run_batched(args, rank: int, world: int, local_rank: int, emit: bool = True)
 # ---------------------------------------------------------------- fused basis
 
 def run_krylov(args, rank: int, world: int, local_rank: int, emit: bool = True):
-    """Config 3b: 100 fp64 vectors of 2^22 values, 32 bits, block 32.  Times
+    """The compressed basis: 100 fp64 vectors of 2^22 values, 32 bits, block 32.  Times
     the fused h = V^T w and y += V c over the compressed basis, against
     decompress-then-torch and against torch on the uncompressed basis."""
     import torch
@@ -920,7 +920,7 @@ def run_krylov(args, rank: int, world: int, local_rank: int, emit: bool = True):
 # ---------------------------------------------------------------- serving
 
 def run_serving(args, rank: int, world: int, local_rank: int, emit: bool = True):
-    """Config 5: a Poisson stream of requests, 60 % compress / 40 % decompress,
+    """The request stream: Poisson arrivals, 60 % compress / 40 % decompress,
     input sizes log-normal (median 1 MB, sigma 1.5, capped at 256 MB), fp32 /
     fp64 50/50, bits from {12, 16, 32}, block 32, 32 GB admission budget.
     Offered load = 70 % of the capacity measured with the same requests all

@@ -104,7 +104,7 @@ def main() -> None:
     x = workloads.normal_np(1 << 20, np.float64, 42)
     comp = oracle.ref_compress(x, 32, 32, canary=0xFF)
     dec = oracle.ref_decompress(comp, x.size, np.float64, 32, 32)
-    out["config1"] = {"dtype": "float64", "n": 1 << 20, "bits": 32, "E": 32, "seed": 42, "canary": 255,
+    out["fp64_2p20_round_trip"] = {"dtype": "float64", "n": 1 << 20, "bits": 32, "E": 32, "seed": 42, "canary": 255,
                       "compressed_sha256": sha(comp), "decompressed_sha256": sha(dec),
                       "compressed_bytes": int(comp.size)}
     with open(os.path.join(HERE, "digests.json"), "w") as f:

@@ -87,10 +87,10 @@ def test_digest_fixtures(cuda):
     assert not bad, f"{len(bad)} mismatches, first: {bad[:8]}"
 
 
-def test_config1_round_trip(cuda):
-    """Config 1: fp64 2^20 N(0,1), E 32, 32 bits -- bytes and values equal the
+def test_fp64_2p20_round_trip(cuda):
+    """The CPU-parity round trip, fp64 2^20 N(0,1), E 32, 32 bits -- bytes and values equal the
     reference's (digests)."""
-    c = json.load(open(os.path.join(GOLDEN, "digests.json")))["config1"]
+    c = json.load(open(os.path.join(GOLDEN, "digests.json")))["fp64_2p20_round_trip"]
     x = workloads.normal_np(c["n"], np.float64, c["seed"])
     comp = gpu_compress(x, 32, 32, canary=0xFF)
     assert _sha(comp) == c["compressed_sha256"]

@@ -92,7 +92,7 @@ def test_zero_code_quirk_fp64():
 # ---------------------------------------------------------------- size algebra
 
 @pytest.mark.parametrize("bits,E,n,expect", [
-    (32, 32, 1 << 20, 4325632),       # config 1: 32768*4 + 256 pad + 32768*128
+    (32, 32, 1 << 20, 4325632),       # fp64 2^20, E 32, 32 bits: 32768*4 + 256 pad + 32768*128
     (16, 32, 512 ** 3, 8388608 + 256 + (1 << 22) * 64),
     (21, 32, 1 << 28, (1 << 23) * 4 + 256 + (1 << 23) * 84),
     (32, 32, 0, 256),                 # empty: a full pad
@@ -156,7 +156,7 @@ def test_digest_fixtures():
         if _sha(comp) != c["compressed_sha256"] or _sha(dec) != c["decompressed_sha256"]:
             bad.append((c["dtype"], c["bits"], c["E"], c["n"]))
     assert not bad, bad[:10]
-    c = d["config1"]
+    c = d["fp64_2p20_round_trip"]
     x = workloads.normal_np(c["n"], np.float64, c["seed"])
     comp = oracle.compress(x, 32, 32, canary=0xFF)
     assert _sha(comp) == c["compressed_sha256"]
