@@ -8,8 +8,9 @@
 // each batch on a free stream slot as soon as one exists, so batches that
 // arrive while others run overlap on the device.  A batch's arrays are
 // grouped by (direction, float type, width) and run through the batched
-// persistent kernels (frsz2_batch_kernels.cuh) from a device descriptor
-// buffer of the slot; arrays those kernels do not take get their own launch.
+// kernels (frsz2_batch_kernels.cuh), one CTA per tile, from a device
+// descriptor buffer and tile index of the slot; arrays those kernels do not
+// take get their own launch.
 // Completion is detected by polling the slot's event; outputs allocated in
 // the arena stay there until released (or are released on completion when
 // the request asks for it).
@@ -121,6 +122,11 @@ struct Slot
   cudaEvent_t join[kSubStreams] = {};
   BatchItem* d_desc = nullptr;
   BatchItem* h_desc = nullptr; // pinned
+  // per tile of the batch's class kernels: the tile's descriptor within its
+  // class (device, and its pinned staging), grown on demand
+  std::uint32_t* d_tmap = nullptr;
+  std::uint32_t* h_tmap = nullptr;
+  std::uint64_t tmap_cap = 0;
   std::vector<Req*> reqs;
   bool busy = false;
 };
@@ -193,7 +199,7 @@ int launch_batch(frsz2_server* sv, Slot& s)
     const int tv = fast_tile_values(is64 ? 8 : 4, kShapes[0].nt, kShapes[0].rpw);
     const Job j = job_of(q, out_ptr(q));
     const void* values = q->r.op == FRSZ2_OP_COMPRESS ? j.values_in : j.values_out;
-    return e.launch != nullptr && q->r.block_size <= tv && fast_eligible(j, is64, values, j.words);
+    return e.launch_tiles != nullptr && q->r.block_size <= tv && fast_eligible(j, is64, values, j.words);
   };
   std::vector<char> is_fast(s.reqs.size());
   for (std::size_t i = 0; i < s.reqs.size(); ++i) {
@@ -222,15 +228,41 @@ int launch_batch(frsz2_server* sv, Slot& s)
           cudaMemcpyAsync(s.d_desc, s.h_desc, used * sizeof(BatchItem), cudaMemcpyHostToDevice, s.stream),
           "descriptor upload"))
       return rc;
-  // class kernels side by side on the slot's sub-streams, each with its
-  // share of the resident CTAs
-  int nclass = 0;
-  std::uint64_t total_tiles = 0;
-  for (int k = 0; k < kKeys; ++k)
-    if (per_key[k]) {
-      ++nclass;
-      total_tiles += tiles[k];
+  // tile index of every class kernel: one CTA per tile reads its descriptor
+  // from it (the slot is idle, so its buffers may be regrown)
+  std::uint64_t tmap_start[kKeys], ntiles = 0;
+  for (int k = 0; k < kKeys; ++k) {
+    tmap_start[k] = ntiles;
+    ntiles += tiles[k];
+  }
+  if (ntiles > s.tmap_cap) {
+    const std::uint64_t cap = std::max<std::uint64_t>(ntiles, 2 * s.tmap_cap);
+    if (s.d_tmap) cudaFree(s.d_tmap);
+    if (s.h_tmap) cudaFreeHost(s.h_tmap);
+    s.d_tmap = nullptr;
+    s.h_tmap = nullptr;
+    s.tmap_cap = 0;
+    if (int rc = cuda_status(cudaMalloc(&s.d_tmap, cap * sizeof(std::uint32_t)), "tile index buffer")) return rc;
+    if (int rc = cuda_status(cudaMallocHost(&s.h_tmap, cap * sizeof(std::uint32_t)), "tile index staging")) return rc;
+    s.tmap_cap = cap;
+  }
+  for (int k = 0; k < kKeys; ++k) {
+    std::uint32_t* m = s.h_tmap + tmap_start[k];
+    for (std::uint64_t d = 0; d < per_key[k]; ++d) {
+      const std::uint64_t t = s.h_desc[start[k] + d].job.tiles;
+      std::fill(m, m + t, (std::uint32_t)d);
+      m += t;
     }
+  }
+  if (ntiles)
+    if (int rc = cuda_status(
+          cudaMemcpyAsync(s.d_tmap, s.h_tmap, ntiles * sizeof(std::uint32_t), cudaMemcpyHostToDevice, s.stream),
+          "tile index upload"))
+      return rc;
+  // class kernels side by side on the slot's sub-streams, one CTA per tile
+  int nclass = 0;
+  for (int k = 0; k < kKeys; ++k)
+    if (per_key[k]) ++nclass;
   const bool fork = nclass > 1;
   if (fork) {
     if (int rc = cuda_status(cudaEventRecord(s.fork, s.stream), "fork")) return rc;
@@ -245,11 +277,8 @@ int launch_batch(frsz2_server* sv, Slot& s)
     const bool is64 = rest >= 65;
     const int bits = rest - (is64 ? 65 : 0);
     const batch_entry e = is64 ? batch_class_f64(bits, 0) : batch_class_f32(bits, 0);
-    const std::uint64_t ctas = (std::uint64_t)sm_count() * (std::uint64_t)e.occupancy(comp);
-    const std::uint64_t share = fork ? (ctas * tiles[k] + total_tiles - 1) / total_tiles : ctas;
-    const unsigned grid = (unsigned)std::max<std::uint64_t>(1, std::min(share, tiles[k]));
     cudaStream_t st = fork ? s.sub[ci++ % kSubStreams] : s.stream;
-    if (int rc = cuda_status(e.launch(comp, s.d_desc + start[k], (int)per_key[k], tiles[k], grid, st),
+    if (int rc = cuda_status(e.launch_tiles(comp, s.d_desc + start[k], s.d_tmap + tmap_start[k], tiles[k], st),
                              "batch launch"))
       return rc;
   }
@@ -544,6 +573,8 @@ void frsz2_server_destroy(frsz2_server* sv)
     }
     if (s.d_desc) cudaFree(s.d_desc);
     if (s.h_desc) cudaFreeHost(s.h_desc);
+    if (s.d_tmap) cudaFree(s.d_tmap);
+    if (s.h_tmap) cudaFreeHost(s.h_tmap);
   }
   if (sv->d_arena) cudaFree(sv->d_arena);
   std::vector<Req*> all;
