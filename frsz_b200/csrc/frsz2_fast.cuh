@@ -881,6 +881,15 @@ __global__ void __launch_bounds__(NT) k_decompress_fast(Job j)
     fast_decompress_tile<T, BITS, NT, RPW, PAD, ESM, MIS>(j, tile);
 }
 
+// The same with registers capped so that 2048 / NT CTAs fit on an SM (more
+// tiles' loads in flight per SM, at the price of some recomputation).
+template<class T, int BITS, int NT, bool PAD>
+__global__ void __launch_bounds__(NT, 2048 / NT) k_decompress_fast_occ(Job j)
+{
+  for (std::uint64_t tile = blockIdx.x; tile < j.tiles; tile += gridDim.x)
+    fast_decompress_tile<T, BITS, NT, 2, PAD>(j, tile);
+}
+
 // Whether a job's exponent blocks end in pad bits (E * bits not a multiple of
 // W); the fast kernels take such jobs only for widths with unaligned segments.
 __host__ __device__ inline bool job_padded(const Job& j)

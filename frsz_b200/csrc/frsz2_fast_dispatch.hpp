@@ -3,16 +3,67 @@
 
 #include "frsz2_fast.cuh"
 
+#include <algorithm>
 #include <array>
 #include <utility>
 
 namespace frsz2b {
+
+// Launch shape of the decompress kernel for a width whose lane segments are
+// not word-aligned (bit 1: 128 threads per CTA instead of 256; bit 0:
+// registers capped for 2048 resident threads per SM), measured per width on
+// B200 at 2^28 (fp64) / 2^29 (fp32) values, blocks of 32 and 64: a shape other
+// than 0 where it gained at least 1 % (up to 29 %, fp32 at 7 bits).  Aligned
+// widths (multiples of 4 bits for fp32, of 8 for fp64) do not use the table.
+template<class T, int BITS>
+constexpr int unaligned_decompress_shape()
+{
+  constexpr signed char f32[33] = { 0, 0, 0, 0, 0, 0, 0, 3, 0, 0, 0, 3, 0, 2, 2, 3, 0,
+                                    2, 2, 3, 0, 0, 3, 2, 0, 2, 2, 2, 0, 2, 2, 2, 0 };
+  constexpr signed char f64[65] = { 0, 0, 0, 0, 1, 3, 3, 3, 0, 0, 0, 3, 0, 3, 3, 3, 0, 0, 0, 3, 0, 3,
+                                    3, 3, 0, 0, 0, 3, 0, 3, 3, 3, 0, 2, 2, 2, 2, 2, 2, 2, 0, 2, 2, 2,
+                                    2, 0, 2, 2, 0, 2, 2, 2, 2, 2, 2, 2, 0, 2, 2, 2, 2, 0, 0, 0, 0 };
+  return sizeof(T) == 8 ? f64[BITS] : f32[BITS];
+}
+
+template<class T, int BITS, int SH>
+cudaError_t launch_decompress_unaligned(const Job& j, cudaStream_t s, unsigned grid)
+{
+  constexpr int NT = (SH & 2) ? 128 : kNT;
+  constexpr int TE = fast_tile_values((int)sizeof(T), NT, 2);
+  Job t = j;
+  if constexpr (NT != kNT) {
+    // tiles of NT / 32 * 2 rows (the caller checked E <= TE)
+    t.tile_blocks = (std::uint32_t)(TE / j.E);
+    t.tiles = (j.n + TE - 1) / TE;
+    grid = (unsigned)std::min<std::uint64_t>(t.tiles, 1u << 30);
+  }
+  const bool pad = job_padded(j);
+  if constexpr ((SH & 1) != 0) {
+    if (pad)
+      k_decompress_fast_occ<T, BITS, NT, true><<<grid, NT, 0, s>>>(t);
+    else
+      k_decompress_fast_occ<T, BITS, NT, false><<<grid, NT, 0, s>>>(t);
+  } else {
+    if (pad)
+      k_decompress_fast<T, BITS, NT, 2, true><<<grid, NT, 0, s>>>(t);
+    else
+      k_decompress_fast<T, BITS, NT, 2, false><<<grid, NT, 0, s>>>(t);
+  }
+  return cudaGetLastError();
+}
 
 // Enqueue the fast compress / decompress kernel for a compile-time width.
 template<class T, int BITS>
 cudaError_t launch_fast_one(bool compress, const Job& j, cudaStream_t s, unsigned grid)
 {
   if constexpr (!fast_cfg<T, BITS>::ALIGNED) {
+    if (!compress) {
+      constexpr int sh = unaligned_decompress_shape<T, BITS>();
+      if ((sh & 2) == 0 || j.E <= fast_tile_values((int)sizeof(T), 128, 2))
+        return launch_decompress_unaligned<T, BITS, sh>(j, s, grid);
+      return launch_decompress_unaligned<T, BITS, sh & 1>(j, s, grid);
+    }
     if (job_padded(j)) {
       if (compress)
         k_compress_fast<T, BITS, kNT, 2, true><<<grid, kNT, 0, s>>>(j);
