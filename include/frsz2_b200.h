@@ -210,7 +210,10 @@ int frsz2_batch_compress_static(const frsz2_batch_item* items, uint64_t count, v
  *   memory of frsz2_basis_workspace_size(m, n) bytes (m sums per slice of
  *   3,072 values), 256-byte aligned, zero on first use (the call leaves it
  *   ready for the next one); the result does not depend on scheduling.  Calls
- *   sharing a workspace must not overlap.
+ *   sharing a workspace must not overlap.  At 64 bits the codes stream
+ *   through shared memory by bulk asynchronous copies; a copy that has not
+ *   landed after 2 s (a device fault, never normal operation) makes every
+ *   h[j] of that call NaN.
  * frsz2_basis_axpy: y[i] += sum_j c[j] * V_j[i] (j in order), c and y device
  *   memory, y 32-byte aligned.
  */
