@@ -834,7 +834,8 @@ def run_batched(args, rank: int, world: int, local_rank: int, emit: bool = True)
 # ---------------------------------------------------------------- fused basis
 
 def run_krylov(args, rank: int, world: int, local_rank: int, emit: bool = True):
-    """The compressed basis: 100 fp64 vectors of 2^22 values, 32 bits, block 32.  Times
+    """The compressed basis: 100 fp64 vectors of 2^22 values, 32 bits (--krylov-bits
+    for the other fused widths), block 32.  Times
     the fused h = V^T w and y += V c over the compressed basis, against
     decompress-then-torch and against torch on the uncompressed basis."""
     import torch
@@ -842,7 +843,7 @@ def run_krylov(args, rank: int, world: int, local_rank: int, emit: bool = True):
     import frsz_b200
 
     torch.cuda.set_device(local_rank)
-    m, n, bits, E = args.krylov_vectors, 1 << 22, 32, 32
+    m, n, bits, E = args.krylov_vectors, 1 << 22, args.krylov_bits, 32
     g = torch.Generator(device="cuda").manual_seed(args.seed + rank)
     V = torch.randn(m, n, generator=g, device="cuda", dtype=torch.float64)
     basis = frsz_b200.CompressedBasis(m, n, bits=bits, block_size=E)
@@ -897,7 +898,8 @@ def run_krylov(args, rank: int, world: int, local_rank: int, emit: bool = True):
         "metric": METRIC, "value": round(value, 3), "unit": "GB/s", "n_gpus": world, "steps": K,
         "warmup": args.warmup, "ms_per_step": round(ms_dot + ms_axpy, 4), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": "krylov100" if m == 100 else f"krylov{m}", "vectors": m, "n": n, "bits": bits,
+        "config": {"workload": ("krylov100" if m == 100 else f"krylov{m}") + ("" if bits == 32 else f"_b{bits}"),
+                   "vectors": m, "n": n, "bits": bits,
                    "block_size": E,
                    "compressed_basis_bytes": comp_bytes, "step": "fused dot h=V^T w, then fused axpy y+=V c"},
         "fused_dot": {"ms": round(ms_dot, 4), "gbs": round(dot_bytes / ms_dot / 1e6, 1),
@@ -1074,6 +1076,8 @@ def main():
     ap.add_argument("--no-batch-autotune", dest="batch_autotune", action="store_false",
                     help="batched4096: keep the plan's default launch shape")
     ap.add_argument("--krylov-vectors", type=int, default=100, help="krylov100: basis size")
+    ap.add_argument("--krylov-bits", type=int, default=32, choices=[16, 21, 24, 32, 48, 64],
+                    help="krylov100: bits per value of the compressed basis")
     ap.add_argument("--streams", type=int, default=4)
     ap.add_argument("--shard", action="store_true",
                     help="split one array across the ranks by block range (strong scaling) instead of one "
