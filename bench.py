@@ -78,6 +78,22 @@ WORKLOADS = {
     "normal_f64_2p25_b21_e32_off1": ("normal", "float64", 1 << 25, 21, 32, 1),
 }
 DEFAULT_WORKLOAD = "loguniform_f64_2p28_b21_e32"
+
+
+def workload_spec(name: str):
+    """A named workload, or any `<normal|loguniform>_<f32|f64>_2p<K>_b<bits>_e<E>`
+    (2^K values, `bits` per value, exponent block E), e.g. normal_f32_2p26_b28_e8."""
+    import re
+
+    if name in WORKLOADS:
+        return WORKLOADS[name]
+    m = re.fullmatch(r"(normal|loguniform)_f(32|64)_2p(\d+)_b(\d+)_e(\d+)", name)
+    if not m:
+        raise SystemExit(f"unknown workload {name}")
+    kind, fb, k, bits, E = m.group(1), m.group(2), int(m.group(3)), int(m.group(4)), int(m.group(5))
+    if not (10 <= k <= 30 and 4 <= bits <= int(fb) and 1 <= E <= 65536):
+        raise SystemExit(f"workload {name} out of range")
+    return (kind, "float32" if fb == "32" else "float64", 1 << k, bits, E)
 # the six cases of the 2 GiB fp64 configuration: (bits, block size)
 F64_2P28_CASES = ((16, 32), (21, 32), (32, 32), (16, 64), (21, 64), (32, 64))
 BATCH_WORKLOADS = ("batched4096", "krylov100", "serving", "legacy_f32_2p28", "legacy_f64_2p27", "legacy_f32_2p25")
@@ -275,7 +291,7 @@ def run_reference_arm(args, rank: int, world: int) -> None:
     one step = compress + decompress of every value, as in our arm."""
     if rank != 0:
         return
-    kind, dtype, n, bits, E = WORKLOADS[args.workload][:5]
+    kind, dtype, n, bits, E = workload_spec(args.workload)[:5]
     threads = os.cpu_count() or 1
     x = make_input_host(kind, dtype, n, args.seed)
     import oracle
@@ -362,13 +378,13 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=torch.device("cuda", local_rank))
 
-    kind, dtype, n, bits, E = WORKLOADS[args.workload][:5]
+    kind, dtype, n, bits, E = workload_spec(args.workload)[:5]
     frsz_b200.lib()  # fail loudly if the library is missing
     x = make_input_cuda(kind, dtype, n, args.seed + rank)
     tdt = x.dtype
     size = frsz_b200.compressed_size(dtype, bits, E, n)
     buf = torch.zeros(size, dtype=torch.uint8, device="cuda")
-    offset = WORKLOADS[args.workload][5] if len(WORKLOADS[args.workload]) > 5 else 0
+    offset = workload_spec(args.workload)[5] if len(workload_spec(args.workload)) > 5 else 0
     if offset:
         xb = torch.empty(n + offset, dtype=tdt, device="cuda")
         xb[offset:] = x
@@ -603,7 +619,7 @@ def run_shard(args, rank: int, world: int, local_rank: int) -> None:
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=torch.device("cuda", local_rank))
-    kind, dtype, n, bits, E = WORKLOADS[args.workload][:5]
+    kind, dtype, n, bits, E = workload_spec(args.workload)[:5]
     frsz_b200.lib()
     x_full = make_input_cuda(kind, dtype, n, args.seed)  # the same array on every rank
     b0, b1 = shard.shard_blocks(n, dtype, bits, E, world, rank)
@@ -1059,7 +1075,9 @@ def main():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS) + list(BATCH_WORKLOADS), default=DEFAULT_WORKLOAD)
+    ap.add_argument("--workload", default=DEFAULT_WORKLOAD,
+                    help="one of %s, %s, or <normal|loguniform>_<f32|f64>_2p<K>_b<bits>_e<E>"
+                    % (", ".join(sorted(WORKLOADS)), ", ".join(BATCH_WORKLOADS)))
     ap.add_argument("--seed", type=int, default=42)
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--cpu-seconds", type=float, default=3.0)

@@ -54,7 +54,8 @@ def test_fp64_every_width(cuda, bits):
 @pytest.mark.parametrize("dtype,E", [(np.float32, e) for e in (8, 16, 64, 128, 512, 1024, 2048, 4096)] +
                          [(np.float64, e) for e in (4, 8, 16, 64, 256, 512, 1024, 2048)])
 def test_block_sizes(cuda, dtype, E):
-    for bits in (8, 12, 16, 21, 24, 32) + ((40, 64) if dtype == np.float64 else ()):
+    # 28 (fp32) and 56 (fp64) bits: seven-word lane segments staged through shared memory
+    for bits in (8, 12, 16, 21, 24, 28, 32) + ((40, 56, 64) if dtype == np.float64 else ()):
         n = 5 * (4096 if dtype == np.float32 else 2048) + 3 * E // 2 + 1
         check(workloads.loguniform_np(n, dtype, seed=E + bits, lo=-20, hi=20), bits, E)
 
