@@ -94,9 +94,12 @@ def workload_spec(name: str):
     if not (10 <= k <= 30 and 4 <= bits <= int(fb) and 1 <= E <= 65536):
         raise SystemExit(f"workload {name} out of range")
     return (kind, "float32" if fb == "32" else "float64", 1 << k, bits, E)
+
+
 # the six cases of the 2 GiB fp64 configuration: (bits, block size)
 F64_2P28_CASES = ((16, 32), (21, 32), (32, 32), (16, 64), (21, 64), (32, 64))
-BATCH_WORKLOADS = ("batched4096", "krylov100", "serving", "legacy_f32_2p28", "legacy_f64_2p27", "legacy_f32_2p25")
+BATCH_WORKLOADS = ("batched4096", "krylov100", "serving", "legacy_f32_2p28", "legacy_f64_2p27", "legacy_f32_2p25",
+                   "plugin_grid")
 
 # DRAM bytes (read + write) per launch from ncu captures, by (workload, kernel);
 # profiles/ holds the captures' summaries and the commands that made them.
@@ -1024,6 +1027,74 @@ def run_serving(args, rank: int, world: int, local_rank: int, emit: bool = True)
     return line
 
 
+def run_plugin_grid(args, rank: int, world: int, local_rank: int) -> None:
+    """Every (block size, bits) the frsz2 plugin offers (src/frsz2.cc:86-129:
+    E = 2 .. 1024 in powers of two, bits 4..32 for fp32 and 4..64 for fp64) on
+    one 1 GiB array of N(0,1) values per float type (2^28 fp32, 2^27 fp64):
+    compress and decompress, each timed over `--steps` launches after
+    `--warmup` untimed ones, as fractions of the measured HBM copy bandwidth.  Prints one summary line (per float type and
+    block size: min / median of each direction and the widths below 0.85); with
+    --grid-rows, every shape."""
+    import torch
+
+    import frsz_b200
+
+    torch.cuda.set_device(local_rank)
+    if rank != 0:
+        return
+    peak = load_peaks()["hbm_gbs"]
+    g = torch.Generator(device="cuda").manual_seed(args.seed)
+    stream = torch.cuda.current_stream()
+    K = max(1, args.steps)
+    rows = []
+    clocks = ClockSampler(torch.cuda.current_device())
+    clocks.start()
+    t0 = time.perf_counter()
+    for dt, tdt, maxb, n in (("float32", torch.float32, 32, 1 << 28), ("float64", torch.float64, 64, 1 << 27)):
+        x = torch.randn(n, generator=g, device="cuda", dtype=tdt)
+        y = torch.empty_like(x)
+        for E in (2, 4, 8, 16, 32, 64, 128, 256, 512, 1024):
+            for bits in range(4, maxb + 1):
+                buf = frsz_b200.compress(x, bits, E)
+                nb = algorithmic_bytes(dt, n, bits, E)
+                frac = []
+                for fn in (lambda: frsz_b200.compress(x, bits, E, out=buf),
+                           lambda: frsz_b200.decompress(buf, n, tdt, bits, E, out=y)):
+                    for _ in range(max(1, args.warmup)):
+                        fn()
+                    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    a.record(stream)
+                    for _ in range(K):
+                        fn()
+                    b.record(stream)
+                    torch.cuda.synchronize()
+                    frac.append(round(nb / (a.elapsed_time(b) / K) / 1e6 / peak, 3))
+                rows.append((dt, E, bits, frac[0], frac[1]))
+                del buf
+        del x, y
+        torch.cuda.empty_cache()
+    summary = {}
+    for dt in ("float32", "float64"):
+        for E in (2, 4, 8, 16, 32, 64, 128, 256, 512, 1024):
+            rs = [r for r in rows if r[0] == dt and r[1] == E]
+            c, d = sorted(r[3] for r in rs), sorted(r[4] for r in rs)
+            summary[f"{dt}_e{E}"] = {"compress_min": c[0], "compress_median": c[len(c) // 2],
+                                     "decompress_min": d[0], "decompress_median": d[len(d) // 2],
+                                     "compress_below_0.85": [r[2] for r in rs if r[3] < 0.85],
+                                     "decompress_below_0.85": [r[2] for r in rs if r[4] < 0.85]}
+    allc, alld = sorted(r[3] for r in rows), sorted(r[4] for r in rows)
+    line = {"metric": METRIC, "workload": "plugin_grid", "shapes": len(rows), "n": {"float32": 1 << 28, "float64": 1 << 27},
+            "steps": K,
+            "of": f"measured HBM copy {peak} GB/s", "data": "synthetic N(0,1)",
+            "compress_median": allc[len(allc) // 2], "decompress_median": alld[len(alld) // 2],
+            "compress_at_least_0.85": sum(v >= 0.85 for v in allc),
+            "decompress_at_least_0.85": sum(v >= 0.85 for v in alld),
+            "wall_s": round(time.perf_counter() - t0, 1), "clocks": clocks.stop(), "by_block_size": summary}
+    if args.grid_rows:
+        line["rows"] = [list(r) for r in rows]
+    print(json.dumps(line), flush=True)
+
+
 def run_legacy(args, rank: int, world: int, local_rank: int) -> None:
     """The legacy "frsz" codec (src/frsz.cc) on N(0,1) data, epsilon 1e-3:
     compress, then decompress as the reference does and with each block's
@@ -1093,6 +1164,7 @@ def main():
     ap.add_argument("--max-batch", type=int, default=256)
     ap.add_argument("--no-batch-autotune", dest="batch_autotune", action="store_false",
                     help="batched4096: keep the plan's default launch shape")
+    ap.add_argument("--grid-rows", action="store_true", help="plugin_grid: print every shape too")
     ap.add_argument("--krylov-vectors", type=int, default=100, help="krylov100: basis size")
     ap.add_argument("--krylov-bits", type=int, default=32, choices=[16, 21, 24, 32, 48, 64],
                     help="krylov100: bits per value of the compressed basis")
@@ -1111,6 +1183,8 @@ def main():
         run_krylov(args, rank, world, local_rank)
     elif args.workload == "serving":
         run_serving(args, rank, world, local_rank)
+    elif args.workload == "plugin_grid":
+        run_plugin_grid(args, rank, world, local_rank)
     elif args.workload.startswith("legacy_"):
         run_legacy(args, rank, world, local_rank)
     elif args.impl == "reference":
