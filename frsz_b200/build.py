@@ -24,7 +24,8 @@ SOURCES = ["frsz2_capi.cu", "frsz2_fast_f32.cu", "frsz2_fast_f64.cu", "frsz2_fas
            "frsz2_batch_f64.cu", "frsz2_batch_static.cu", "frsz2_krylov.cu",
            "frsz2_serve.cu", "frsz1_legacy.cu", "frsz2_blockwise_f32.cu", "frsz2_blockwise_f64.cu",
            "frsz2_fast_mis_f32.cu", "frsz2_fast_mis_f64.cu",
-           "frsz2_blockvec_f32.cu", "frsz2_blockvec_f64.cu", "frsz2_chunked_f32.cu", "frsz2_chunked_f64.cu"] + \
+           "frsz2_blockvec_f32.cu", "frsz2_blockvec_f64.cu", "frsz2_chunked_f32.cu", "frsz2_chunked_f64.cu",
+           "frsz2_fast_gen_f32.cu", "frsz2_fast_gen_f64.cu"] + \
           [f"frsz2_bwc_{t}_e{e}.cu" for t in ("f64", "f32") for e in (3, 5, 6, 7, 12)]
 OBJDIR = os.path.join(HERE, "_build")
 

@@ -138,6 +138,16 @@ static cudaError_t try_fast(bool compress, const Job& j, cudaStream_t s)
   if (fast_mis_eligible(j, sizeof(T) == 8, values, j.words))
     return sizeof(T) == 8 ? launch_fast_mis_f64(j.bits, compress, j, s, grid)
                           : launch_fast_mis_f32(j.bits, compress, j, s, grid);
+  if (const std::uint32_t tb = fast_gen_tile_blocks(j, sizeof(T) == 8, values, j.words)) {
+    // block sizes that are a multiple of a lane's values: tiles of tb whole blocks
+    Job t = j;
+    const std::uint64_t tv = (std::uint64_t)tb * (std::uint64_t)j.E;
+    t.tile_blocks = tb;
+    t.tiles = (j.n + tv - 1) / tv;
+    const unsigned g = (unsigned)std::min<std::uint64_t>(t.tiles, 1u << 30);
+    return sizeof(T) == 8 ? launch_fast_gen_f64(j.bits, compress, t, s, g)
+                          : launch_fast_gen_f32(j.bits, compress, t, s, g);
+  }
   return cudaErrorNotSupported;
 }
 

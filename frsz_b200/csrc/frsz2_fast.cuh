@@ -479,9 +479,14 @@ __device__ __forceinline__ void load_lane_exps(const std::uint8_t* p, std::int64
 // stage_words<>::value words, 16-byte aligned.
 // more_tiles: whether the CTA runs another tile after this one (the shared
 // block maxima are then reused, so their readers must be done first).
-template<class T, int BITS, int NT, int RPW_, bool PAD = false, int ESM = 0, bool MIS = false>
+// GEN: blocks of a multiple E of P values that is not a power of two, without
+// block padding (as for fast_decompress_tile): tiles of j.tile_blocks whole
+// blocks; each lane's maxima go to s_gmax (2 * ROWS * 32 words), and after
+// one barrier a lane takes its block's maxima from its block's E / P lanes.
+template<class T, int BITS, int NT, int RPW_, bool PAD = false, int ESM = 0, bool MIS = false, bool GEN = false>
 __device__ __forceinline__ void fast_compress_tile(const Job& j, std::uint64_t tile, std::uint32_t* s_rmax,
-                                                   std::uint32_t* s_stage, bool more_tiles = true)
+                                                   std::uint32_t* s_stage, bool more_tiles = true,
+                                                   std::uint32_t* s_gmax = nullptr, std::uint32_t mE = 0)
 {
   using Cfg = fast_cfg<T, BITS, NT, RPW_, ESM>;
   using U = typename Cfg::U;
@@ -497,11 +502,12 @@ __device__ __forceinline__ void fast_compress_tile(const Job& j, std::uint64_t t
   const int TB = (int)j.tile_blocks;
 
   {
-    const std::uint64_t e0 = tile * (std::uint64_t)TE;
+    const int TV = GEN ? TB * E : TE; // values of a whole tile
+    const std::uint64_t e0 = tile * (std::uint64_t)TV;
     const std::uint64_t rem64 = j.n - e0;
-    const bool full = rem64 >= (std::uint64_t)TE;
-    const int rem = full ? TE : (int)rem64;
-    const int nbt = full ? TB : ((rem + E - 1) >> log2E);
+    const bool full = rem64 >= (std::uint64_t)TV;
+    const int rem = full ? TV : (int)rem64;
+    const int nbt = full ? TB : GEN ? (rem + E - 1) / E : ((rem + E - 1) >> log2E);
     const std::uint64_t b0 = tile * (std::uint64_t)TB;
 
     // MIS: values off the 32-byte layout by kw words (whole tiles only)
@@ -510,7 +516,7 @@ __device__ __forceinline__ void fast_compress_tile(const Job& j, std::uint64_t t
 #pragma unroll
     for (int rr = 0; rr < RPW; ++rr) {
       const int idx = (rr * Cfg::WARPS + warp) * ROW + lane * P;
-      if (MIS ? full : (full || idx + P <= rem)) {
+      if (GEN ? idx + P <= rem : MIS ? full : (full || idx + P <= rem)) {
         std::uint32_t v[8];
         if constexpr (MIS)
           ld_lane_mis<Cfg::ALIGNED>(reinterpret_cast<const std::uint32_t*>(x + e0 + idx) - kw, kw, e0 + idx == 0, v);
@@ -554,7 +560,31 @@ __device__ __forceinline__ void fast_compress_tile(const Job& j, std::uint64_t t
         kc[rr] = km[rr];
       }
     }
-    if (G <= 32) {
+    if constexpr (GEN) {
+      // a block is G consecutive lanes of the tile, across warps and rows
+#pragma unroll
+      for (int rr = 0; rr < RPW; ++rr) {
+        const int t = (rr * Cfg::WARPS + warp) * 32 + lane;
+        s_gmax[t] = km[rr];
+        s_gmax[Cfg::ROWS * 32 + t] = kc[rr];
+      }
+      __syncthreads();
+#pragma unroll
+      for (int rr = 0; rr < RPW; ++rr) {
+        const int idx = (rr * Cfg::WARPS + warp) * ROW + lane * P;
+        if (idx < rem) {
+          const int l0 = (int)__umulhi((unsigned)idx, mE) * G;
+          std::uint32_t a = 0, b = 0;
+          for (int q = 0; q < G; ++q) {
+            a = max(a, s_gmax[l0 + q]);
+            b = max(b, s_gmax[Cfg::ROWS * 32 + l0 + q]);
+          }
+          km[rr] = a;
+          kc[rr] = b;
+        }
+      }
+      if (more_tiles) __syncthreads();
+    } else if (G <= 32) {
       for (int s = 1; s < G; s <<= 1) {
 #pragma unroll
         for (int rr = 0; rr < RPW; ++rr) km[rr] = max(km[rr], __shfl_xor_sync(0xFFFFFFFFu, km[rr], s));
@@ -610,7 +640,7 @@ __device__ __forceinline__ void fast_compress_tile(const Job& j, std::uint64_t t
     for (int rr = 0; rr < RPW; ++rr) {
       const int row = rr * Cfg::WARPS + warp;
       const int idx = row * ROW + lane * P;
-      const int bl = idx >> log2E;
+      const int bl = GEN ? (int)__umulhi((unsigned)idx, mE) : idx >> log2E;
       C c[P];
       if constexpr (ESM == 0) {
         const int field = (int)(kc[rr] >> K::FSHIFT);
@@ -625,7 +655,7 @@ __device__ __forceinline__ void fast_compress_tile(const Job& j, std::uint64_t t
 #pragma unroll
           for (int i = 0; i < P; ++i) c[i] = (C)to_code<T>(u[rr][i], (std::int16_t)be, BITS);
         }
-        if ((idx & (E - 1)) == 0 && bl < nbt)
+        if ((GEN ? idx == bl * E : (idx & (E - 1)) == 0) && bl < nbt)
           store_word(j.exps + (b0 + (std::uint64_t)bl) * (std::uint64_t)(W / 8), (std::uint64_t)be, W);
       } else {
         // the lane's P / ESM blocks, each with its own exponent
@@ -676,7 +706,7 @@ __device__ __forceinline__ void fast_compress_tile(const Job& j, std::uint64_t t
         for (int q = lane; q < L / 4; q += 32) {
           const std::uint32_t off = row_byte + 16u * (std::uint32_t)q;
           const uint4 v = st4[q];
-          if (full || off + 16u <= wb) {
+          if ((full && !GEN) || off + 16u <= wb) {
             __stcs(reinterpret_cast<uint4*>(dst + off), v);
           } else if (off < wb) {
             const std::uint32_t vw[4] = { v.x, v.y, v.z, v.w };
@@ -691,7 +721,7 @@ __device__ __forceinline__ void fast_compress_tile(const Job& j, std::uint64_t t
         std::uint32_t out[NW];
 #pragma unroll
         for (int i = 0; i < NW; ++i) out[i] = seg[i];
-        if (full || off + 4u * NW <= wb) {
+        if ((full && !GEN) || off + 4u * NW <= wb) {
           store_words<NW>(reinterpret_cast<std::uint32_t*>(dst + off), out);
         } else {
 #pragma unroll
@@ -757,7 +787,7 @@ __device__ __forceinline__ void fast_compress_tile(const Job& j, std::uint64_t t
         for (int q = lane; q < (PAD ? (int)(row_bytes >> 4) : L / 4); q += 32) {
           const std::uint32_t off = row_byte + 16u * (std::uint32_t)q;
           const uint4 v = st4[q];
-          if (full || off + 16u <= wb) {
+          if ((full && !GEN) || off + 16u <= wb) {
             __stcs(reinterpret_cast<uint4*>(dst + off), v);
           } else if (off < wb) {
             const std::uint32_t vw[4] = { v.x, v.y, v.z, v.w };
@@ -772,20 +802,28 @@ __device__ __forceinline__ void fast_compress_tile(const Job& j, std::uint64_t t
   }
 }
 
-template<class T, int BITS, int NT = kNT, int RPW = 2, bool PAD = false, int ESM = 0, bool MIS = false>
+template<class T, int BITS, int NT = kNT, int RPW = 2, bool PAD = false, int ESM = 0, bool MIS = false,
+         bool GEN = false>
 __global__ void __launch_bounds__(NT) k_compress_fast(Job j)
 {
   __shared__ std::uint32_t s_rmax[2 * fast_cfg<T, BITS, NT, RPW>::ROWS];
   __shared__ __align__(16) std::uint32_t s_stage[stage_words<T, BITS, NT, RPW, ESM>::value];
+  __shared__ std::uint32_t s_gmax[GEN ? 2 * fast_cfg<T, BITS, NT, RPW>::ROWS * 32 : 1];
+  const std::uint32_t mE = GEN ? 0xFFFFFFFFu / (std::uint32_t)j.E + 1u : 0u; // ceil(2^32 / E), E not a power of two
   for (std::uint64_t tile = blockIdx.x; tile < j.tiles; tile += gridDim.x)
-    fast_compress_tile<T, BITS, NT, RPW, PAD, ESM, MIS>(j, tile, s_rmax, s_stage, tile + gridDim.x < j.tiles);
+    fast_compress_tile<T, BITS, NT, RPW, PAD, ESM, MIS, GEN>(j, tile, s_rmax, s_stage, tile + gridDim.x < j.tiles,
+                                                             s_gmax, mE);
 }
 
 // ---------------------------------------------------------------- decompress
 
 // One tile of decompress.
-template<class T, int BITS, int NT, int RPW_, bool PAD = false, int ESM = 0, bool MIS = false>
-__device__ __forceinline__ void fast_decompress_tile(const Job& j, std::uint64_t tile)
+// GEN: exponent blocks of any multiple E of a lane's P values (not a power of
+// two), without block padding: a tile is j.tile_blocks whole blocks (rows past
+// them idle), a lane's P values lie in one block, found as idx / E with a
+// multiply-high by mE = ceil(2^32 / E) (exact for idx, E < 2^12).
+template<class T, int BITS, int NT, int RPW_, bool PAD = false, int ESM = 0, bool MIS = false, bool GEN = false>
+__device__ __forceinline__ void fast_decompress_tile(const Job& j, std::uint64_t tile, std::uint32_t mE = 0)
 {
   using Cfg = fast_cfg<T, BITS, NT, RPW_, ESM>;
   constexpr int NBL = ESM ? Cfg::P / ESM : 1; // exponents per lane
@@ -801,10 +839,11 @@ __device__ __forceinline__ void fast_decompress_tile(const Job& j, std::uint64_t
   const std::uint32_t blk_bits = 8u * j.block_bytes;
 
   {
-    const std::uint64_t e0 = tile * (std::uint64_t)TE;
+    const int TV = GEN ? TB * E : TE; // values of a whole tile
+    const std::uint64_t e0 = tile * (std::uint64_t)TV;
     const std::uint64_t rem64 = j.n - e0;
-    const bool full = rem64 >= (std::uint64_t)TE;
-    const int rem = full ? TE : (int)rem64;
+    const bool full = rem64 >= (std::uint64_t)TV;
+    const int rem = full ? TV : (int)rem64;
     const std::uint64_t b0 = tile * (std::uint64_t)TB;
     const std::uint32_t* __restrict__ src =
       reinterpret_cast<const std::uint32_t*>(j.words + b0 * (std::uint64_t)j.block_bytes);
@@ -815,8 +854,9 @@ __device__ __forceinline__ void fast_decompress_tile(const Job& j, std::uint64_t
     for (int rr = 0; rr < RPW; ++rr) {
       const int row = rr * Cfg::WARPS + warp;
       const int idx = row * ROW + lane * P;
-      if (!full && idx >= rem) continue;
-      const std::uint8_t* ep = j.exps + (b0 + (std::uint64_t)(idx >> log2E)) * (std::uint64_t)(W / 8);
+      if ((GEN || !full) && idx >= rem) continue;
+      const int bl = GEN ? (int)__umulhi((unsigned)idx, mE) : idx >> log2E;
+      const std::uint8_t* ep = j.exps + (b0 + (std::uint64_t)bl) * (std::uint64_t)(W / 8);
       if constexpr (ESM == 0)
         be[rr][0] = load_exp(ep, W);
       else
@@ -847,7 +887,7 @@ __device__ __forceinline__ void fast_decompress_tile(const Job& j, std::uint64_t
     for (int rr = 0; rr < RPW; ++rr) {
       const int row = rr * Cfg::WARPS + warp;
       const int idx = row * ROW + lane * P;
-      if (!full && idx >= rem) continue;
+      if ((GEN || !full) && idx >= rem) continue;
       std::uint32_t seg[NW + 1];
       if constexpr (Cfg::ALIGNED) {
 #pragma unroll
@@ -906,11 +946,13 @@ __device__ __forceinline__ void fast_decompress_tile(const Job& j, std::uint64_t
   }
 }
 
-template<class T, int BITS, int NT = kNT, int RPW = 2, bool PAD = false, int ESM = 0, bool MIS = false>
+template<class T, int BITS, int NT = kNT, int RPW = 2, bool PAD = false, int ESM = 0, bool MIS = false,
+         bool GEN = false>
 __global__ void __launch_bounds__(NT) k_decompress_fast(Job j)
 {
+  const std::uint32_t mE = GEN ? 0xFFFFFFFFu / (std::uint32_t)j.E + 1u : 0u; // ceil(2^32 / E), E not a power of two
   for (std::uint64_t tile = blockIdx.x; tile < j.tiles; tile += gridDim.x)
-    fast_decompress_tile<T, BITS, NT, RPW, PAD, ESM, MIS>(j, tile);
+    fast_decompress_tile<T, BITS, NT, RPW, PAD, ESM, MIS, GEN>(j, tile, mE);
 }
 
 // The same with registers capped so that 2048 / NT CTAs fit on an SM (more
@@ -944,6 +986,27 @@ __host__ inline bool fast_eligible(const Job& j, int dtype_is_f64, const void* v
   if (reinterpret_cast<std::uintptr_t>(values) % 32 != 0) return false;
   if (reinterpret_cast<std::uintptr_t>(words) % 32 != 0) return false;
   return true;
+}
+
+// Whole blocks per tile of the GEN decompress instances, or 0 when they do not
+// apply: a block size that is a multiple of a lane's P values but not a power
+// of two, at most a tile, no block padding, 32-byte aligned pointers.  The
+// count is the most whole blocks a tile holds, rounded down so that every
+// tile's words start on a 32-byte boundary.
+__host__ inline std::uint32_t fast_gen_tile_blocks(const Job& j, int dtype_is_f64, const void* values,
+                                                   const void* words)
+{
+  const int P = dtype_is_f64 ? 4 : 8;
+  const int TE = dtype_is_f64 ? 2048 : 4096;
+  const int E = j.E;
+  if (E < P || E > TE || E % P != 0 || (E & (E - 1)) == 0) return 0;
+  if (((std::uint64_t)E * (std::uint64_t)j.bits) % (std::uint64_t)j.W != 0) return 0;
+  if (reinterpret_cast<std::uintptr_t>(values) % 32 != 0) return 0;
+  if (reinterpret_cast<std::uintptr_t>(words) % 32 != 0) return 0;
+  std::uint32_t g = 32; // blocks per 32-byte period of the word stream
+  for (std::uint32_t b = j.block_bytes; g > 1 && b % 2 == 0; b /= 2) g /= 2;
+  const std::uint32_t tb = (std::uint32_t)(TE / E) / g * g;
+  return tb;
 }
 
 // Requirements of the MIS instances: those of the fast kernels, with the

@@ -99,6 +99,38 @@ constexpr auto make_fast_table(std::integer_sequence<int, I...>)
 cudaError_t launch_fast_f32(int bits, bool compress, const Job& j, cudaStream_t s, unsigned grid);
 cudaError_t launch_fast_f64(int bits, bool compress, const Job& j, cudaStream_t s, unsigned grid);
 
+// Blocks whose size is a multiple of a lane's values but not a power of two
+// (fast_gen_tile_blocks; the caller sets the Job's whole-block tiles).
+template<class T, int BITS>
+cudaError_t launch_fast_gen_one(bool compress, const Job& j, cudaStream_t s, unsigned grid)
+{
+  if (compress) {
+    // a lane reads its block's E / P lane maxima: up to 32 of them
+    if (j.E > 32 * fast_cfg<T, BITS>::P) return cudaErrorNotSupported;
+    k_compress_fast<T, BITS, kNT, 2, false, 0, false, true><<<grid, kNT, 0, s>>>(j);
+  } else {
+    k_decompress_fast<T, BITS, kNT, 2, false, 0, false, true><<<grid, kNT, 0, s>>>(j);
+  }
+  return cudaGetLastError();
+}
+
+template<class T, int LO, int... I>
+constexpr auto make_fast_gen_table(std::integer_sequence<int, I...>)
+{
+  return std::array<fast_fn, sizeof...(I)>{ &launch_fast_gen_one<T, LO + I>... };
+}
+
+#define FRSZ2_FAST_GEN_TABLE(T, LO, HI, NAME)                                                                       \
+  cudaError_t NAME(int bits, bool compress, const Job& j, cudaStream_t s, unsigned grid)                          \
+  {                                                                                                                \
+    static constexpr auto table = make_fast_gen_table<T, LO>(std::make_integer_sequence<int, HI - LO + 1>{});      \
+    if (bits < LO || bits > HI) return cudaErrorNotSupported;                                                      \
+    return table[bits - LO](compress, j, s, grid);                                                                 \
+  }
+
+cudaError_t launch_fast_gen_f32(int bits, bool compress, const Job& j, cudaStream_t s, unsigned grid);
+cudaError_t launch_fast_gen_f64(int bits, bool compress, const Job& j, cudaStream_t s, unsigned grid);
+
 // The same kernels for a values pointer off the 32-byte layout (MIS).
 template<class T, int BITS>
 cudaError_t launch_fast_mis_one(bool compress, const Job& j, cudaStream_t s, unsigned grid)
