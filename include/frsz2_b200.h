@@ -28,9 +28,11 @@
  * 32-byte aligned buffer run at about the HBM bandwidth; values off the
  * 32-byte layout (a view such as x + 1) at 0.7-0.9 of it; block sizes 3, 5, 6,
  * 7 and 12 at 0.74-1.0, other block sizes up to 16 values at 0.4-0.8; block
- * sizes 17-128 decompress at 0.33-0.89 and compress at 0.2-0.7; larger block
- * sizes that are not powers of two, or a buffer off the 32-byte layout, on
- * slower general kernels.
+ * sizes that are a multiple of 8 (fp32) / 4 (fp64) values without block
+ * padding decompress at about the HBM bandwidth and compress at 0.75-1.0 (up
+ * to 256 / 128 values); other block sizes of 17-128 values decompress at
+ * 0.33-0.89 and compress at 0.2-0.7; larger block sizes that are not powers of
+ * two, or a buffer off the 32-byte layout, on slower general kernels.
  */
 #ifndef FRSZ2_B200_H
 #define FRSZ2_B200_H
