@@ -819,9 +819,10 @@ __global__ void __launch_bounds__(NT) k_compress_fast(Job j)
 
 // One tile of decompress.
 // GEN: exponent blocks of any multiple E of a lane's P values (not a power of
-// two), without block padding: a tile is j.tile_blocks whole blocks (rows past
-// them idle), a lane's P values lie in one block, found as idx / E with a
-// multiply-high by mE = ceil(2^32 / E) (exact for idx, E < 2^12).
+// two): a tile is j.tile_blocks whole blocks (rows past them idle), a lane's P
+// values lie in one block, found as idx / E with a multiply-high by
+// mE = ceil(2^32 / E) (exact for idx, E < 2^12).  With PAD (unaligned widths
+// only) a lane's stream bit is block * block bits + (idx - block * E) * BITS.
 template<class T, int BITS, int NT, int RPW_, bool PAD = false, int ESM = 0, bool MIS = false, bool GEN = false>
 __device__ __forceinline__ void fast_decompress_tile(const Job& j, std::uint64_t tile, std::uint32_t mE = 0)
 {
@@ -865,6 +866,7 @@ __device__ __forceinline__ void fast_decompress_tile(const Job& j, std::uint64_t
       // multiple of W; only the unaligned widths take padded blocks; blocks
       // smaller than a lane are padded at compile-time positions)
       const std::uint32_t S = ESM ? (std::uint32_t)(idx / (ESM ? ESM : 1)) * Cfg::BBB
+                              : (PAD && GEN) ? (std::uint32_t)bl * blk_bits + (std::uint32_t)(idx - bl * E) * BITS
                               : PAD ? (std::uint32_t)(idx >> log2E) * blk_bits + (std::uint32_t)(idx & (E - 1)) * BITS
                                     : (std::uint32_t)idx * BITS;
       if constexpr (Cfg::ALIGNED) {
@@ -893,7 +895,9 @@ __device__ __forceinline__ void fast_decompress_tile(const Job& j, std::uint64_t
 #pragma unroll
         for (int i = 0; i <= NW; ++i) seg[i] = wv[rr][i];
       } else {
+        const int blg = (PAD && GEN) ? (int)__umulhi((unsigned)idx, mE) : 0;
         const int o = (int)((ESM ? (std::uint32_t)(idx / (ESM ? ESM : 1)) * Cfg::BBB
+                             : (PAD && GEN) ? (std::uint32_t)blg * blk_bits + (std::uint32_t)(idx - blg * E) * BITS
                              : PAD ? (std::uint32_t)(idx >> log2E) * blk_bits + (std::uint32_t)(idx & (E - 1)) * BITS
                                    : (std::uint32_t)idx * BITS) &
                             31u);
@@ -988,11 +992,12 @@ __host__ inline bool fast_eligible(const Job& j, int dtype_is_f64, const void* v
   return true;
 }
 
-// Whole blocks per tile of the GEN decompress instances, or 0 when they do not
-// apply: a block size that is a multiple of a lane's P values but not a power
-// of two, at most a tile, no block padding, 32-byte aligned pointers.  The
-// count is the most whole blocks a tile holds, rounded down so that every
-// tile's words start on a 32-byte boundary.
+// Whole blocks per tile of the GEN instances, or 0 when they do not apply: a
+// block size that is a multiple of a lane's P values but not a power of two,
+// at most a tile, 32-byte aligned pointers (padded blocks: decompress of the
+// unaligned widths only, checked at launch).  The count is the most whole
+// blocks a tile holds, rounded down so that every tile's words start on a
+// 32-byte boundary.
 __host__ inline std::uint32_t fast_gen_tile_blocks(const Job& j, int dtype_is_f64, const void* values,
                                                    const void* words)
 {
@@ -1000,7 +1005,6 @@ __host__ inline std::uint32_t fast_gen_tile_blocks(const Job& j, int dtype_is_f6
   const int TE = dtype_is_f64 ? 2048 : 4096;
   const int E = j.E;
   if (E < P || E > TE || E % P != 0 || (E & (E - 1)) == 0) return 0;
-  if (((std::uint64_t)E * (std::uint64_t)j.bits) % (std::uint64_t)j.W != 0) return 0;
   if (reinterpret_cast<std::uintptr_t>(values) % 32 != 0) return 0;
   if (reinterpret_cast<std::uintptr_t>(words) % 32 != 0) return 0;
   std::uint32_t g = 32; // blocks per 32-byte period of the word stream

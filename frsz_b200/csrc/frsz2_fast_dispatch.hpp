@@ -104,10 +104,18 @@ cudaError_t launch_fast_f64(int bits, bool compress, const Job& j, cudaStream_t 
 template<class T, int BITS>
 cudaError_t launch_fast_gen_one(bool compress, const Job& j, cudaStream_t s, unsigned grid)
 {
+  const bool pad = job_padded(j);
   if (compress) {
-    // a lane reads its block's E / P lane maxima: up to 32 of them
-    if (j.E > 32 * fast_cfg<T, BITS>::P) return cudaErrorNotSupported;
+    // a lane reads its block's E / P lane maxima: up to 32 of them; padded
+    // blocks keep the other kernels
+    if (pad || j.E > 32 * fast_cfg<T, BITS>::P) return cudaErrorNotSupported;
     k_compress_fast<T, BITS, kNT, 2, false, 0, false, true><<<grid, kNT, 0, s>>>(j);
+  } else if (pad) {
+    // padded blocks: lanes place their bits by stream position (unaligned widths)
+    if constexpr (fast_cfg<T, BITS>::ALIGNED)
+      return cudaErrorNotSupported;
+    else
+      k_decompress_fast<T, BITS, kNT, 2, true, 0, false, true><<<grid, kNT, 0, s>>>(j);
   } else {
     k_decompress_fast<T, BITS, kNT, 2, false, 0, false, true><<<grid, kNT, 0, s>>>(j);
   }
