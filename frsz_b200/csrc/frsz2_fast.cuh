@@ -574,10 +574,13 @@ __device__ __forceinline__ void fast_compress_tile(const Job& j, std::uint64_t t
         const int idx = (rr * Cfg::WARPS + warp) * ROW + lane * P;
         if (idx < rem) {
           const int l0 = (int)__umulhi((unsigned)idx, mE) * G;
-          std::uint32_t a = 0, b = 0;
-          for (int q = 0; q < G; ++q) {
-            a = max(a, s_gmax[l0 + q]);
-            b = max(b, s_gmax[Cfg::ROWS * 32 + l0 + q]);
+          std::uint32_t a = 0;
+          for (int q = 0; q < G; ++q) a = max(a, s_gmax[l0 + q]);
+          // the clean maxima differ from the raw ones only in blocks with an Inf or NaN
+          std::uint32_t b = a;
+          if (a >= K::SPECIAL) {
+            b = 0;
+            for (int q = 0; q < G; ++q) b = max(b, s_gmax[Cfg::ROWS * 32 + l0 + q]);
           }
           km[rr] = a;
           kc[rr] = b;

@@ -118,15 +118,17 @@ def test_nan_inf(cuda, dtype):
     x[rng.choice(n, 10, replace=False)] = np.inf
     x[rng.choice(n, 10, replace=False)] = -np.inf
     for bits in ((8, 16, 21, 32) if dtype == np.float32 else (8, 16, 21, 32, 40, 64)):
-        for E in (8, 32):
+        # 24 and 48: block sizes that are a multiple of a lane's values (maxima through shared memory)
+        for E in (8, 32, 24, 48):
             check(x, bits, E)
 
 
 @pytest.mark.parametrize("E", [3, 5, 6, 7, 12, 48, 100, 257, 1000, 2047])
 def test_block_sizes_not_powers_of_two(cuda, E):
-    """Block sizes the fast kernels do not take (one-thread-per-block kernels
-    up to 16, chunked and warp-per-block kernels above): several chunks, a
-    partial last block, special values."""
+    """Block sizes that are not powers of two (one-thread-per-block kernels up
+    to 16, whole-block tiles of the fast kernels for multiples of a lane's
+    values, chunked and warp-per-block kernels for the rest): several chunks,
+    a partial last block, special values."""
     for dtype, widths in ((np.float32, (4, 9, 16, 21, 32)), (np.float64, (5, 8, 21, 33, 52, 64))):
         n = 3 * 2048 + 2 * E + E // 2 + 1
         x = special_values(dtype, n, E)
