@@ -826,11 +826,15 @@ __global__ void __launch_bounds__(NT) k_compress_fast(Job j)
 // values lie in one block, found as idx / E with a multiply-high by
 // mE = ceil(2^32 / E) (exact for idx, E < 2^12).  With PAD (unaligned widths
 // only) a lane's stream bit is block * block bits + (idx - block * E) * BITS.
-template<class T, int BITS, int NT, int RPW_, bool PAD = false, int ESM = 0, bool MIS = false, bool GEN = false>
+// HALF (with GEN, blocks without padding): E is a multiple of P / 2 but not of
+// P, so a lane's two halves may lie in two blocks; each half takes its own
+// exponent.
+template<class T, int BITS, int NT, int RPW_, bool PAD = false, int ESM = 0, bool MIS = false, bool GEN = false,
+         bool HALF = false>
 __device__ __forceinline__ void fast_decompress_tile(const Job& j, std::uint64_t tile, std::uint32_t mE = 0)
 {
   using Cfg = fast_cfg<T, BITS, NT, RPW_, ESM>;
-  constexpr int NBL = ESM ? Cfg::P / ESM : 1; // exponents per lane
+  constexpr int NBL = ESM ? Cfg::P / ESM : HALF ? 2 : 1; // exponents per lane
   using U = typename Cfg::U;
   using C = typename Cfg::C;
   constexpr int P = Cfg::P, L = Cfg::L, NW = Cfg::NW, ROW = Cfg::ROW, RPW = Cfg::RPW, TE = Cfg::TE,
@@ -861,10 +865,15 @@ __device__ __forceinline__ void fast_decompress_tile(const Job& j, std::uint64_t
       if ((GEN || !full) && idx >= rem) continue;
       const int bl = GEN ? (int)__umulhi((unsigned)idx, mE) : idx >> log2E;
       const std::uint8_t* ep = j.exps + (b0 + (std::uint64_t)bl) * (std::uint64_t)(W / 8);
-      if constexpr (ESM == 0)
+      if constexpr (ESM == 0) {
         be[rr][0] = load_exp(ep, W);
-      else
+        if constexpr (HALF) {
+          const int bl1 = (int)__umulhi((unsigned)(idx + P / 2), mE);
+          be[rr][1] = load_exp(j.exps + (b0 + (std::uint64_t)bl1) * (std::uint64_t)(W / 8), W);
+        }
+      } else {
         load_lane_exps<W, NBL>(ep, be[rr]);
+      }
       // tile stream bit (blocks may end in pad bits when E * BITS is not a
       // multiple of W; only the unaligned widths take padded blocks; blocks
       // smaller than a lane are padded at compile-time positions)
@@ -954,12 +963,12 @@ __device__ __forceinline__ void fast_decompress_tile(const Job& j, std::uint64_t
 }
 
 template<class T, int BITS, int NT = kNT, int RPW = 2, bool PAD = false, int ESM = 0, bool MIS = false,
-         bool GEN = false>
+         bool GEN = false, bool HALF = false>
 __global__ void __launch_bounds__(NT) k_decompress_fast(Job j)
 {
   const std::uint32_t mE = GEN ? 0xFFFFFFFFu / (std::uint32_t)j.E + 1u : 0u; // ceil(2^32 / E), E not a power of two
   for (std::uint64_t tile = blockIdx.x; tile < j.tiles; tile += gridDim.x)
-    fast_decompress_tile<T, BITS, NT, RPW, PAD, ESM, MIS, GEN>(j, tile, mE);
+    fast_decompress_tile<T, BITS, NT, RPW, PAD, ESM, MIS, GEN, HALF>(j, tile, mE);
 }
 
 // The same with registers capped so that 2048 / NT CTAs fit on an SM (more
@@ -996,7 +1005,7 @@ __host__ inline bool fast_eligible(const Job& j, int dtype_is_f64, const void* v
 }
 
 // Whole blocks per tile of the GEN instances, or 0 when they do not apply: a
-// block size that is a multiple of a lane's P values but not a power of two,
+// block size that is a multiple of half a lane's P values but not a power of two,
 // at most a tile, 32-byte aligned pointers (padded blocks: decompress of the
 // unaligned widths only, checked at launch).  The count is the most whole
 // blocks a tile holds, rounded down so that every tile's words start on a
@@ -1007,11 +1016,13 @@ __host__ inline std::uint32_t fast_gen_tile_blocks(const Job& j, int dtype_is_f6
   const int P = dtype_is_f64 ? 4 : 8;
   const int TE = dtype_is_f64 ? 2048 : 4096;
   const int E = j.E;
-  if (E < P || E > TE || E % P != 0 || (E & (E - 1)) == 0) return 0;
+  if (E < P || E > TE || E % (P / 2) != 0 || (E & (E - 1)) == 0) return 0;
   if (reinterpret_cast<std::uintptr_t>(values) % 32 != 0) return 0;
   if (reinterpret_cast<std::uintptr_t>(words) % 32 != 0) return 0;
   std::uint32_t g = 32; // blocks per 32-byte period of the word stream
   for (std::uint32_t b = j.block_bytes; g > 1 && b % 2 == 0; b /= 2) g /= 2;
+  // E a multiple of P / 2 only: an even block count keeps tiles whole lanes
+  if (E % P != 0 && g < 2) g = 2;
   const std::uint32_t tb = (std::uint32_t)(TE / E) / g * g;
   return tb;
 }

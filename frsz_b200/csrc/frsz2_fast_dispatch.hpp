@@ -105,6 +105,12 @@ template<class T, int BITS>
 cudaError_t launch_fast_gen_one(bool compress, const Job& j, cudaStream_t s, unsigned grid)
 {
   const bool pad = job_padded(j);
+  if (j.E % fast_cfg<T, BITS>::P != 0) {
+    // a multiple of half a lane: decompress of blocks without padding only
+    if (compress || pad) return cudaErrorNotSupported;
+    k_decompress_fast<T, BITS, kNT, 2, false, 0, false, true, true><<<grid, kNT, 0, s>>>(j);
+    return cudaGetLastError();
+  }
   if (compress) {
     // a lane reads its block's E / P lane maxima: up to 32 of them; padded
     // blocks keep the other kernels

@@ -60,12 +60,13 @@ def test_block_sizes(cuda, dtype, E):
         check(workloads.loguniform_np(n, dtype, seed=E + bits, lo=-20, hi=20), bits, E)
 
 
-@pytest.mark.parametrize("dtype,E", [(np.float32, e) for e in (24, 40, 48, 56, 72, 96, 120, 1000)] +
-                         [(np.float64, e) for e in (12, 20, 24, 36, 48, 100, 1000, 2044)])
+@pytest.mark.parametrize("dtype,E", [(np.float32, e) for e in (24, 40, 48, 56, 72, 96, 120, 1000, 12, 20, 100)] +
+                         [(np.float64, e) for e in (12, 20, 24, 36, 48, 100, 1000, 2044, 6, 10, 18, 102)])
 def test_block_sizes_multiple_of_a_lane(cuda, dtype, E):
-    """Block sizes that are a multiple of a lane's values but not a power of
-    two: whole-block tiles (padded blocks at 13, 21, 33 and 37 bits: decompress
-    only), with a partial last block and a partial last tile."""
+    """Block sizes that are a multiple of a lane's values, or of half of them
+    (fp32 12 / 20 / 100, fp64 6 / 10 / 18 / 102: decompress only), but not a
+    power of two: whole-block tiles (padded blocks at 13, 21, 33 and 37 bits:
+    decompress only), with a partial last block and a partial last tile."""
     te = 4096 if dtype == np.float32 else 2048
     for bits in (8, 12, 13, 16, 20, 21, 24, 32) + ((33, 37, 40, 48, 64) if dtype == np.float64 else ()):
         n = 3 * te + 7 * E // 2 + 5
