@@ -483,7 +483,10 @@ __device__ __forceinline__ void load_lane_exps(const std::uint8_t* p, std::int64
 // block padding (as for fast_decompress_tile): tiles of j.tile_blocks whole
 // blocks; each lane's maxima go to s_gmax (2 * ROWS * 32 words), and after
 // one barrier a lane takes its block's maxima from its block's E / P lanes.
-template<class T, int BITS, int NT, int RPW_, bool PAD = false, int ESM = 0, bool MIS = false, bool GEN = false>
+// HALF (with GEN): E a multiple of P / 2 but not of P; the same per half lane
+// (s_gmax of 4 * ROWS * 32 words), each half encoding with its own exponent.
+template<class T, int BITS, int NT, int RPW_, bool PAD = false, int ESM = 0, bool MIS = false, bool GEN = false,
+         bool HALF = false>
 __device__ __forceinline__ void fast_compress_tile(const Job& j, std::uint64_t tile, std::uint32_t* s_rmax,
                                                    std::uint32_t* s_stage, bool more_tiles = true,
                                                    std::uint32_t* s_gmax = nullptr, std::uint32_t mE = 0)
@@ -538,7 +541,50 @@ __device__ __forceinline__ void fast_compress_tile(const Job& j, std::uint64_t t
     // block maxima: raw keys detect Inf/NaN, clean keys skip NaN like std::max
     // (blocks within a lane, ESM > 0: computed per block below)
     std::uint32_t km[RPW], kc[RPW];
-    if constexpr (ESM == 0) {
+    std::uint32_t kmh[RPW][2], kch[RPW][2]; // HALF: per half lane
+    if constexpr (HALF) {
+      constexpr int H = P / 2;
+      const int G2 = E / H; // half lanes per block
+#pragma unroll
+      for (int rr = 0; rr < RPW; ++rr) {
+        const int t = ((rr * Cfg::WARPS + warp) * 32 + lane) * 2;
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          std::uint32_t m = K::raw(u[rr][h * H]);
+#pragma unroll
+          for (int i = 1; i < H; ++i) m = max(m, K::raw(u[rr][h * H + i]));
+          std::uint32_t cm = m;
+          if (m >= K::SPECIAL) {
+            cm = K::clean(u[rr][h * H]);
+#pragma unroll
+            for (int i = 1; i < H; ++i) cm = max(cm, K::clean(u[rr][h * H + i]));
+          }
+          s_gmax[t + h] = m;
+          s_gmax[2 * Cfg::ROWS * 32 + t + h] = cm;
+        }
+      }
+      __syncthreads();
+#pragma unroll
+      for (int rr = 0; rr < RPW; ++rr) {
+        const int idx = (rr * Cfg::WARPS + warp) * ROW + lane * P;
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          std::uint32_t a = 0, bmax = 0;
+          if (idx + h * H < rem) {
+            const int l0 = (int)__umulhi((unsigned)(idx + h * H), mE) * G2;
+            for (int q = 0; q < G2; ++q) a = max(a, s_gmax[l0 + q]);
+            bmax = a;
+            if (a >= K::SPECIAL) {
+              bmax = 0;
+              for (int q = 0; q < G2; ++q) bmax = max(bmax, s_gmax[2 * Cfg::ROWS * 32 + l0 + q]);
+            }
+          }
+          kmh[rr][h] = a;
+          kch[rr][h] = bmax;
+        }
+      }
+      if (more_tiles) __syncthreads();
+    } else if constexpr (ESM == 0) {
     bool any_special = false;
 #pragma unroll
     for (int rr = 0; rr < RPW; ++rr) {
@@ -645,7 +691,27 @@ __device__ __forceinline__ void fast_compress_tile(const Job& j, std::uint64_t t
       const int idx = row * ROW + lane * P;
       const int bl = GEN ? (int)__umulhi((unsigned)idx, mE) : idx >> log2E;
       C c[P];
-      if constexpr (ESM == 0) {
+      if constexpr (HALF) {
+        constexpr int H = P / 2;
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int field = (int)(kch[rr][h] >> K::FSHIFT);
+          const std::int64_t ex = exponent_of_field<T>(field);
+          const std::int64_t be = wrap_signed(ex, W);
+          const bool plain = kmh[rr][h] < K::SPECIAL && be == ex && plain_exponent<T>(be);
+          if (plain) {
+            const T scale = pow2<T>(BITS - 2 - (int)be);
+#pragma unroll
+            for (int i = h * H; i < (h + 1) * H; ++i) c[i] = encode_plain<T, BITS>(u[rr][i], scale);
+          } else {
+#pragma unroll
+            for (int i = h * H; i < (h + 1) * H; ++i) c[i] = (C)to_code<T>(u[rr][i], (std::int16_t)be, BITS);
+          }
+          const int bh = (int)__umulhi((unsigned)(idx + h * H), mE);
+          if (idx + h * H == bh * E && bh < nbt)
+            store_word(j.exps + (b0 + (std::uint64_t)bh) * (std::uint64_t)(W / 8), (std::uint64_t)be, W);
+        }
+      } else if constexpr (ESM == 0) {
         const int field = (int)(kc[rr] >> K::FSHIFT);
         const std::int64_t ex = exponent_of_field<T>(field);
         const std::int64_t be = wrap_signed(ex, W);
@@ -806,16 +872,16 @@ __device__ __forceinline__ void fast_compress_tile(const Job& j, std::uint64_t t
 }
 
 template<class T, int BITS, int NT = kNT, int RPW = 2, bool PAD = false, int ESM = 0, bool MIS = false,
-         bool GEN = false>
+         bool GEN = false, bool HALF = false>
 __global__ void __launch_bounds__(NT) k_compress_fast(Job j)
 {
   __shared__ std::uint32_t s_rmax[2 * fast_cfg<T, BITS, NT, RPW>::ROWS];
   __shared__ __align__(16) std::uint32_t s_stage[stage_words<T, BITS, NT, RPW, ESM>::value];
-  __shared__ std::uint32_t s_gmax[GEN ? 2 * fast_cfg<T, BITS, NT, RPW>::ROWS * 32 : 1];
+  __shared__ std::uint32_t s_gmax[GEN ? (HALF ? 4 : 2) * fast_cfg<T, BITS, NT, RPW>::ROWS * 32 : 1];
   const std::uint32_t mE = GEN ? 0xFFFFFFFFu / (std::uint32_t)j.E + 1u : 0u; // ceil(2^32 / E), E not a power of two
   for (std::uint64_t tile = blockIdx.x; tile < j.tiles; tile += gridDim.x)
-    fast_compress_tile<T, BITS, NT, RPW, PAD, ESM, MIS, GEN>(j, tile, s_rmax, s_stage, tile + gridDim.x < j.tiles,
-                                                             s_gmax, mE);
+    fast_compress_tile<T, BITS, NT, RPW, PAD, ESM, MIS, GEN, HALF>(j, tile, s_rmax, s_stage,
+                                                                   tile + gridDim.x < j.tiles, s_gmax, mE);
 }
 
 // ---------------------------------------------------------------- decompress

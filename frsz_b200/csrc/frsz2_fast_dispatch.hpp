@@ -106,9 +106,17 @@ cudaError_t launch_fast_gen_one(bool compress, const Job& j, cudaStream_t s, uns
 {
   const bool pad = job_padded(j);
   if (j.E % fast_cfg<T, BITS>::P != 0) {
-    // a multiple of half a lane: decompress of blocks without padding only
-    if (compress || pad) return cudaErrorNotSupported;
-    k_decompress_fast<T, BITS, kNT, 2, false, 0, false, true, true><<<grid, kNT, 0, s>>>(j);
+    // a multiple of half a lane, blocks without padding: two exponents per
+    // lane; compress reads up to 32 half-lane maxima per block, and blocks of
+    // up to 16 values keep the one-thread-per-block kernels (measured faster:
+    // fp64 16 bits E 6 1.04 against 0.67 of HBM, fp32 16 bits E 12 0.82 / 0.69)
+    if (pad) return cudaErrorNotSupported;
+    if (compress) {
+      if (j.E <= 16 || j.E > 16 * fast_cfg<T, BITS>::P) return cudaErrorNotSupported;
+      k_compress_fast<T, BITS, kNT, 2, false, 0, false, true, true><<<grid, kNT, 0, s>>>(j);
+    } else {
+      k_decompress_fast<T, BITS, kNT, 2, false, 0, false, true, true><<<grid, kNT, 0, s>>>(j);
+    }
     return cudaGetLastError();
   }
   if (compress) {
