@@ -30,7 +30,8 @@
  * 7 and 12 at 0.74-1.0, other block sizes up to 16 values at 0.4-0.8; block
  * sizes that are a multiple of 8 (fp32) / 4 (fp64) values without block
  * padding decompress at about the HBM bandwidth and compress at 0.75-1.0 (up
- * to 256 / 128 values); other block sizes of 17-128 values decompress at
+ * to 256 / 128 values), multiples of 4 / 2 decompress at about the HBM
+ * bandwidth and compress at 0.55-0.7; other block sizes of 17-128 values decompress at
  * 0.33-0.89 and compress at 0.2-0.7; larger block sizes that are not powers of
  * two, or a buffer off the 32-byte layout, on slower general kernels.
  */
