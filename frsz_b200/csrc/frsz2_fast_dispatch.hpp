@@ -99,8 +99,10 @@ constexpr auto make_fast_table(std::integer_sequence<int, I...>)
 cudaError_t launch_fast_f32(int bits, bool compress, const Job& j, cudaStream_t s, unsigned grid);
 cudaError_t launch_fast_f64(int bits, bool compress, const Job& j, cudaStream_t s, unsigned grid);
 
-// Blocks whose size is a multiple of a lane's values but not a power of two
-// (fast_gen_tile_blocks; the caller sets the Job's whole-block tiles).
+// Blocks whose size is a multiple of a lane's values, or of half of them, but
+// not a power of two (fast_gen_tile_blocks; the caller sets the Job's
+// whole-block tiles).  cudaErrorNotSupported sends the job to the other
+// kernels.
 template<class T, int BITS>
 cudaError_t launch_fast_gen_one(bool compress, const Job& j, cudaStream_t s, unsigned grid)
 {
