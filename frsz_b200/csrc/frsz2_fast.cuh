@@ -485,8 +485,11 @@ __device__ __forceinline__ void load_lane_exps(const std::uint8_t* p, std::int64
 // one barrier a lane takes its block's maxima from its block's E / P lanes.
 // HALF (with GEN): E a multiple of P / 2 but not of P; the same per half lane
 // (s_gmax of 4 * ROWS * 32 words), each half encoding with its own exponent.
+// WCR: blocks of exactly RPW warp rows (power-of-two E = RPW * 32 * P); a
+// warp's rows are consecutive (row = warp * RPW + rr), so a block lies in one
+// warp and its maximum needs no barrier.
 template<class T, int BITS, int NT, int RPW_, bool PAD = false, int ESM = 0, bool MIS = false, bool GEN = false,
-         bool HALF = false>
+         bool HALF = false, bool WCR = false>
 __device__ __forceinline__ void fast_compress_tile(const Job& j, std::uint64_t tile, std::uint32_t* s_rmax,
                                                    std::uint32_t* s_stage, bool more_tiles = true,
                                                    std::uint32_t* s_gmax = nullptr, std::uint32_t mE = 0)
@@ -518,7 +521,7 @@ __device__ __forceinline__ void fast_compress_tile(const Job& j, std::uint64_t t
     U u[RPW][P];
 #pragma unroll
     for (int rr = 0; rr < RPW; ++rr) {
-      const int idx = (rr * Cfg::WARPS + warp) * ROW + lane * P;
+      const int idx = (WCR ? warp * RPW + rr : rr * Cfg::WARPS + warp) * ROW + lane * P;
       if (GEN ? idx + P <= rem : MIS ? full : (full || idx + P <= rem)) {
         std::uint32_t v[8];
         if constexpr (MIS)
@@ -606,7 +609,20 @@ __device__ __forceinline__ void fast_compress_tile(const Job& j, std::uint64_t t
         kc[rr] = km[rr];
       }
     }
-    if constexpr (GEN) {
+    if constexpr (WCR) {
+      // the block is this warp's RPW rows
+      std::uint32_t a = 0, c = 0;
+#pragma unroll
+      for (int rr = 0; rr < RPW; ++rr) {
+        a = max(a, __reduce_max_sync(0xFFFFFFFFu, km[rr]));
+        c = max(c, __reduce_max_sync(0xFFFFFFFFu, kc[rr]));
+      }
+#pragma unroll
+      for (int rr = 0; rr < RPW; ++rr) {
+        km[rr] = a;
+        kc[rr] = c;
+      }
+    } else if constexpr (GEN) {
       // a block is G consecutive lanes of the tile, across warps and rows
 #pragma unroll
       for (int rr = 0; rr < RPW; ++rr) {
@@ -687,7 +703,7 @@ __device__ __forceinline__ void fast_compress_tile(const Job& j, std::uint64_t t
 
 #pragma unroll
     for (int rr = 0; rr < RPW; ++rr) {
-      const int row = rr * Cfg::WARPS + warp;
+      const int row = WCR ? warp * RPW + rr : rr * Cfg::WARPS + warp;
       const int idx = row * ROW + lane * P;
       const int bl = GEN ? (int)__umulhi((unsigned)idx, mE) : idx >> log2E;
       C c[P];
@@ -872,7 +888,7 @@ __device__ __forceinline__ void fast_compress_tile(const Job& j, std::uint64_t t
 }
 
 template<class T, int BITS, int NT = kNT, int RPW = 2, bool PAD = false, int ESM = 0, bool MIS = false,
-         bool GEN = false, bool HALF = false>
+         bool GEN = false, bool HALF = false, bool WCR = false>
 __global__ void __launch_bounds__(NT) k_compress_fast(Job j)
 {
   __shared__ std::uint32_t s_rmax[2 * fast_cfg<T, BITS, NT, RPW>::ROWS];
@@ -880,8 +896,8 @@ __global__ void __launch_bounds__(NT) k_compress_fast(Job j)
   __shared__ std::uint32_t s_gmax[GEN ? (HALF ? 4 : 2) * fast_cfg<T, BITS, NT, RPW>::ROWS * 32 : 1];
   const std::uint32_t mE = GEN ? 0xFFFFFFFFu / (std::uint32_t)j.E + 1u : 0u; // ceil(2^32 / E), E not a power of two
   for (std::uint64_t tile = blockIdx.x; tile < j.tiles; tile += gridDim.x)
-    fast_compress_tile<T, BITS, NT, RPW, PAD, ESM, MIS, GEN, HALF>(j, tile, s_rmax, s_stage,
-                                                                   tile + gridDim.x < j.tiles, s_gmax, mE);
+    fast_compress_tile<T, BITS, NT, RPW, PAD, ESM, MIS, GEN, HALF, WCR>(j, tile, s_rmax, s_stage,
+                                                                        tile + gridDim.x < j.tiles, s_gmax, mE);
 }
 
 // ---------------------------------------------------------------- decompress
