@@ -649,7 +649,14 @@ __device__ __forceinline__ void fast_compress_tile(const Job& j, std::uint64_t t
         }
       }
       if (more_tiles) __syncthreads();
-    } else if (G <= 32) {
+    } else if (G == 32) {
+      // a block is one warp row: one warp-wide reduction per row
+#pragma unroll
+      for (int rr = 0; rr < RPW; ++rr) {
+        km[rr] = __reduce_max_sync(0xFFFFFFFFu, km[rr]);
+        kc[rr] = warp_special ? __reduce_max_sync(0xFFFFFFFFu, kc[rr]) : km[rr];
+      }
+    } else if (G < 32) {
       for (int s = 1; s < G; s <<= 1) {
 #pragma unroll
         for (int rr = 0; rr < RPW; ++rr) km[rr] = max(km[rr], __shfl_xor_sync(0xFFFFFFFFu, km[rr], s));

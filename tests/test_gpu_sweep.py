@@ -120,9 +120,9 @@ def test_nan_inf(cuda, dtype):
     x[rng.choice(n, 10, replace=False)] = -np.inf
     for bits in ((8, 16, 21, 32) if dtype == np.float32 else (8, 16, 21, 32, 40, 64)):
         # 24, 48 (and 20: half a lane for fp32): block sizes that are not powers of
-        # two, with block maxima through shared memory; 256 / 512: blocks of two
-        # warp rows (fp64 / fp32), maxima within a warp
-        for E in (8, 32, 24, 48, 20, 256, 512):
+        # two, with block maxima through shared memory; 128 / 256 / 512: blocks of
+        # one or two warp rows, maxima by warp reductions
+        for E in (8, 32, 24, 48, 20, 128, 256, 512):
             check(x, bits, E)
 
 
